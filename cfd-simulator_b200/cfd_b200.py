@@ -1,0 +1,417 @@
+"""Python binding of the B200 SIMPLE solver's C ABI (include/cfd_gpu.h,
+include/cfd_mesh.h), over ctypes.
+
+The names mirror the reference's C++ interface so host code reads the same:
+``SimpleSolver.create(mesh, conditions, settings)``, ``set_turbulence_model``,
+``initialise``, ``iterate``, ``field``, ``mass_flux``, ``divergence``,
+``set_settings`` (include/cfd/solver/SimpleSolver.hpp:159-274). Arrays are
+numpy float64 in the reference's ordering (cells j*cellsI + i; faces j-faces
+then i-faces; Vec2 arrays as (x, y) pairs).
+
+The library is the in-tree ``libcfd_b200.so`` built by ``make`` in this
+directory; importing this module fails loudly when it is missing. There is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libcfd_b200.so")
+
+if not os.path.exists(LIBRARY_PATH):
+    raise ImportError(
+        f"{LIBRARY_PATH} is missing: build it with `make -C {_HERE}` (needs nvcc); "
+        "the solver has no CPU fallback")
+_lib = C.CDLL(LIBRARY_PATH)
+
+# ---- status codes (ErrorCode + 1) --------------------------------------------
+OK = 0
+ERROR_NAMES = {1: "InvalidArgument", 2: "OutOfRange", 3: "NotFound", 4: "IoFailure",
+               5: "NotImplemented", 6: "InitializationFailure", 7: "NumericalFailure",
+               8: "Internal"}
+
+BC_INTERNAL, BC_INLET, BC_OUTLET, BC_FARFIELD, BC_NOSLIP_WALL = range(5)
+FACE_INTERIOR, FACE_WALL, FACE_FARFIELD, FACE_OUTLET, FACE_WAKECUT = range(5)
+
+FIELDS = ["U", "V", "P", "RHO", "MU_EFF", "MASS_FLUX", "DIVERGENCE", "MU_MOLECULAR",
+          "GRAD_U", "GRAD_V", "GRAD_P", "MOM_DIAG", "MOM_SOURCE_U", "MOM_SOURCE_V",
+          "MOM_UPPER", "MOM_LOWER", "MOMENTUM_DIAGONAL", "P_DIAG", "P_SOURCE", "P_UPPER",
+          "NET_FLUX", "P_CORRECTION", "K", "OMEGA", "MUT", "WALL_DISTANCE", "STRAIN", "F1",
+          "F2", "CROSS_DIFFUSION", "PRODUCTION", "GRAD_K", "GRAD_OMEGA", "T_DIAG_K",
+          "T_SOURCE_K", "T_DIAG_W", "T_SOURCE_W"]
+FIELD = {name: k for k, name in enumerate(FIELDS)}
+FACE_FIELDS = {"MASS_FLUX", "MOM_UPPER", "MOM_LOWER", "P_UPPER"}
+VEC2_FIELDS = {"GRAD_U", "GRAD_V", "GRAD_P", "GRAD_K", "GRAD_OMEGA"}
+
+STAGES = ["GRADIENTS", "MOMENTUM_ASSEMBLY", "MOMENTUM_SOLVE", "RHIE_CHOW",
+          "PRESSURE_ASSEMBLY", "PRESSURE_SOLVE", "CORRECT", "SST_BLENDING", "SST_ASSEMBLY",
+          "SST_SOLVE", "END"]
+STAGE = {name: k for k, name in enumerate(STAGES)}
+
+MODEL_NONE, MODEL_LAMINAR, MODEL_SST = 0, 1, 2
+
+
+class CfdError(RuntimeError):
+    """A non-zero cfd_status, with the library's message."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def _check(code: int) -> None:
+    if code != OK:
+        raise CfdError(code, _lib.cfd_last_error().decode())
+
+
+# ---- C structs ------------------------------------------------------------------
+class MeshDesc(C.Structure):
+    _fields_ = [("nodes_i", C.c_int), ("nodes_j", C.c_int), ("cell_count", C.c_int),
+                ("face_count", C.c_int), ("cell_centroids", C.c_void_p),
+                ("cell_areas", C.c_void_p), ("face_centres", C.c_void_p),
+                ("face_normals", C.c_void_p), ("face_areas", C.c_void_p),
+                ("face_owner", C.c_void_p), ("face_neighbour", C.c_void_p),
+                ("face_boundary", C.c_void_p), ("face_partner", C.c_void_p)]
+
+
+class FaceBc(C.Structure):
+    _fields_ = [("kind", C.c_void_p), ("velocity", C.c_void_p), ("pressure", C.c_void_p)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("velocity_relaxation", C.c_double), ("pressure_relaxation", C.c_double),
+                ("momentum_sweeps", C.c_int), ("pressure_iterations", C.c_int),
+                ("pressure_tolerance", C.c_double), ("scheme", C.c_int),
+                ("turbulence_relaxation", C.c_double), ("inflow_intensity", C.c_double),
+                ("inflow_viscosity_ratio", C.c_double), ("inflow_length_scale", C.c_double),
+                ("non_orthogonal_correctors", C.c_int), ("non_orthogonal_blend", C.c_double),
+                ("precision", C.c_int)]
+
+    @staticmethod
+    def defaults(**overrides) -> "Settings":
+        s = Settings()
+        _lib.cfd_default_settings(C.byref(s))
+        for key, value in overrides.items():
+            setattr(s, key, value)
+        return s
+
+    def packed(self) -> np.ndarray:
+        """The 12-value layout the oracle and the reference harness take."""
+        return np.array([self.velocity_relaxation, self.pressure_relaxation, self.momentum_sweeps,
+                         self.pressure_iterations, self.pressure_tolerance, self.scheme,
+                         self.turbulence_relaxation, self.inflow_intensity,
+                         self.inflow_viscosity_ratio, self.inflow_length_scale,
+                         self.non_orthogonal_correctors, self.non_orthogonal_blend], np.float64)
+
+
+MONITOR_FIELDS = ["continuity", "momentum_x", "momentum_y", "mass_imbalance", "max_divergence",
+                  "pressure_iterations", "turbulence_first", "turbulence_second", "min_energy",
+                  "max_energy", "min_dissipation", "max_dissipation", "min_eddy_viscosity",
+                  "max_eddy_viscosity", "max_eddy_viscosity_ratio", "max_wall_yplus"]
+
+
+class Monitor(C.Structure):
+    _fields_ = [("continuity", C.c_double), ("momentum_x", C.c_double),
+                ("momentum_y", C.c_double), ("mass_imbalance", C.c_double),
+                ("max_divergence", C.c_double), ("pressure_iterations", C.c_int),
+                ("pad_", C.c_int), ("turbulence_first", C.c_double),
+                ("turbulence_second", C.c_double), ("min_energy", C.c_double),
+                ("max_energy", C.c_double), ("min_dissipation", C.c_double),
+                ("max_dissipation", C.c_double), ("min_eddy_viscosity", C.c_double),
+                ("max_eddy_viscosity", C.c_double), ("max_eddy_viscosity_ratio", C.c_double),
+                ("max_wall_yplus", C.c_double)]
+
+    def as_array(self) -> np.ndarray:
+        return np.array([float(getattr(self, name)) for name in MONITOR_FIELDS])
+
+    def worst(self) -> float:
+        """ResidualSet::worst (FlowField.cpp:49-51)."""
+        return max(abs(self.continuity), abs(self.momentum_x), abs(self.momentum_y))
+
+
+class CGridOptions(C.Structure):
+    _fields_ = [("upstream_chords", C.c_double), ("downstream_chords", C.c_double),
+                ("vertical_chords", C.c_double), ("surface_points", C.c_int),
+                ("wake_points", C.c_int), ("normal_points", C.c_int),
+                ("first_layer_height", C.c_double), ("normal_blend_length", C.c_double),
+                ("normal_smoothing_passes", C.c_int)]
+
+
+def _sig(name, restype, *argtypes):
+    fn = getattr(_lib, name)
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+    return fn
+
+
+_P = C.c_void_p
+_sig("cfd_last_error", C.c_char_p)
+_sig("cfd_default_settings", None, _P)
+_sig("cfd_gpu_create", C.c_int, _P, _P, _P, _P)
+_sig("cfd_gpu_set_turbulence", C.c_int, _P, C.c_int)
+_sig("cfd_gpu_initialise", C.c_int, _P, _P, _P, _P, _P, _P)
+_sig("cfd_gpu_iterate", C.c_int, _P, C.c_int, _P, _P)
+_sig("cfd_gpu_converge", C.c_int, _P, C.c_int, C.c_double, _P, _P)
+_sig("cfd_gpu_iterate_partial", C.c_int, _P, C.c_int, _P)
+_sig("cfd_gpu_read_field", C.c_int, _P, C.c_int, _P)
+_sig("cfd_gpu_load_state", C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P)
+_sig("cfd_gpu_set_settings", C.c_int, _P, _P)
+_sig("cfd_gpu_dims", C.c_int, _P, _P)
+_sig("cfd_gpu_scalars", C.c_int, _P, _P)
+_sig("cfd_gpu_destroy", C.c_int, _P)
+_sig("cfd_default_cgrid_options", None, _P)
+_sig("cfd_mesh_cgrid", C.c_int, C.c_char_p, _P, _P)
+_sig("cfd_mesh_box", C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+     C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int, _P)
+_sig("cfd_mesh_describe", C.c_int, _P, _P)
+_sig("cfd_mesh_nodes", _P, _P)
+_sig("cfd_mesh_face_conditions", C.c_int, _P, C.c_double, C.c_double, _P, _P, _P)
+_sig("cfd_mesh_free", None, _P)
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---- meshes -----------------------------------------------------------------------
+@dataclass
+class MeshArrays:
+    """A face-based structured mesh (cfd::mesh::Mesh's arrays)."""
+    nodes_i: int
+    nodes_j: int
+    centroid: np.ndarray
+    cell_area: np.ndarray
+    face_centre: np.ndarray
+    face_normal: np.ndarray
+    face_area: np.ndarray
+    owner: np.ndarray
+    neighbour: np.ndarray
+    boundary: np.ndarray
+    partner: np.ndarray
+    nodes: np.ndarray | None = None
+
+    @property
+    def cells(self) -> int:
+        return int(self.cell_area.size)
+
+    @property
+    def faces(self) -> int:
+        return int(self.face_area.size)
+
+    @property
+    def cells_i(self) -> int:
+        return self.nodes_i - 1
+
+    @property
+    def cells_j(self) -> int:
+        return self.nodes_j - 1
+
+    def desc(self) -> MeshDesc:
+        d = MeshDesc()
+        d.nodes_i, d.nodes_j = self.nodes_i, self.nodes_j
+        d.cell_count, d.face_count = self.cells, self.faces
+        for name, arr in (("cell_centroids", self.centroid), ("cell_areas", self.cell_area),
+                          ("face_centres", self.face_centre), ("face_normals", self.face_normal),
+                          ("face_areas", self.face_area), ("face_owner", self.owner),
+                          ("face_neighbour", self.neighbour), ("face_boundary", self.boundary),
+                          ("face_partner", self.partner)):
+            setattr(d, name, arr.ctypes.data)
+        return d
+
+
+def _take_mesh(handle: C.c_void_p) -> MeshArrays:
+    d = MeshDesc()
+    _check(_lib.cfd_mesh_describe(handle, C.byref(d)))
+    n, f = d.cell_count, d.face_count
+
+    def dbl(ptr, count):
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_double)), (count,)).copy()
+
+    def i32(ptr, count):
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int)), (count,)).copy()
+
+    nodes_ptr = _lib.cfd_mesh_nodes(handle)
+    mesh = MeshArrays(d.nodes_i, d.nodes_j, dbl(d.cell_centroids, 2 * n), dbl(d.cell_areas, n),
+                      dbl(d.face_centres, 2 * f), dbl(d.face_normals, 2 * f), dbl(d.face_areas, f),
+                      i32(d.face_owner, f), i32(d.face_neighbour, f), i32(d.face_boundary, f),
+                      i32(d.face_partner, f), dbl(nodes_ptr, 2 * d.nodes_i * d.nodes_j))
+    return mesh
+
+
+def default_cgrid_options(**overrides) -> CGridOptions:
+    o = CGridOptions()
+    _lib.cfd_default_cgrid_options(C.byref(o))
+    for key, value in overrides.items():
+        setattr(o, key, value)
+    return o
+
+
+def cgrid(designation: str, **options) -> MeshArrays:
+    """generateCGrid for a closed-trailing-edge NACA section of chord 1."""
+    opts = default_cgrid_options(**options)
+    handle = C.c_void_p()
+    _check(_lib.cfd_mesh_cgrid(designation.encode(), C.byref(opts), C.byref(handle)))
+    try:
+        return _take_mesh(handle)
+    finally:
+        _lib.cfd_mesh_free(handle)
+
+
+def box(length=1.0, height=1.0, cells_x=40, cells_y=20, grading=0, first_cell_height=0.01,
+        left=FACE_FARFIELD, right=FACE_OUTLET, lower=FACE_WALL, upper=FACE_WALL,
+        origin_x=0.0, origin_y=0.0) -> MeshArrays:
+    """generateBox (BoxGrid.cpp)."""
+    handle = C.c_void_p()
+    _check(_lib.cfd_mesh_box(origin_x, origin_y, length, height, cells_x, cells_y, grading,
+                             first_cell_height, left, right, lower, upper, C.byref(handle)))
+    try:
+        return _take_mesh(handle)
+    finally:
+        _lib.cfd_mesh_free(handle)
+
+
+@dataclass
+class FaceConditions:
+    kind: np.ndarray      # int32 per face
+    velocity: np.ndarray  # 2 per face
+    pressure: np.ndarray  # per face
+
+    def struct(self) -> FaceBc:
+        return FaceBc(self.kind.ctypes.data, self.velocity.ctypes.data, self.pressure.ctypes.data)
+
+
+def freestream_velocity(speed: float, alpha_deg: float) -> tuple[float, float]:
+    """FreestreamConditions::velocity (Freestream.cpp:11-14), with libm's cos/sin."""
+    alpha = alpha_deg * math.pi / 180.0
+    return speed * math.cos(alpha), speed * math.sin(alpha)
+
+
+def freestream_conditions(mesh: MeshArrays, speed: float, alpha_deg: float) -> FaceConditions:
+    """buildFaceConditions with the default BoundaryConditions
+    (BoundaryConditions.cpp:73-97): wall -> no-slip, far field -> FarField,
+    outlet -> Outlet, interior and wake cut -> Internal; pressure 0."""
+    if not (math.isfinite(speed) and speed > 0):
+        raise CfdError(1, "freestream speed must be positive")
+    ux, uy = freestream_velocity(speed, alpha_deg)
+    table = np.full(8, BC_INTERNAL, np.int32)
+    table[FACE_WALL], table[FACE_FARFIELD], table[FACE_OUTLET] = BC_NOSLIP_WALL, BC_FARFIELD, BC_OUTLET
+    kind = table[mesh.boundary].astype(np.int32)
+    vel = np.zeros((mesh.faces, 2))
+    vel[kind != BC_NOSLIP_WALL] = (ux, uy)
+    return FaceConditions(kind, vel.reshape(-1).copy(), np.zeros(mesh.faces))
+
+
+def uniform_field(mesh: MeshArrays, speed: float, alpha_deg: float, density: float,
+                  reynolds: float, chord: float = 1.0):
+    """FlowField::uniform (FlowField.cpp:21-47): (u, v, p, rho, mu)."""
+    ux, uy = freestream_velocity(speed, alpha_deg)
+    n = mesh.cells
+    mu = density * speed * chord / reynolds
+    return (np.full(n, ux), np.full(n, uy), np.zeros(n), np.full(n, density), np.full(n, mu))
+
+
+# ---- solver ------------------------------------------------------------------------
+class SimpleSolver:
+    """A device-resident steady SIMPLE solve (SimpleSolver.hpp:159-274)."""
+
+    def __init__(self, handle: C.c_void_p, mesh: MeshArrays):
+        self._h = handle
+        self.mesh = mesh
+
+    @classmethod
+    def create(cls, mesh: MeshArrays, conditions: FaceConditions,
+               settings: Settings | None = None) -> "SimpleSolver":
+        desc = mesh.desc()
+        bc = conditions.struct()
+        handle = C.c_void_p()
+        _check(_lib.cfd_gpu_create(C.byref(desc), C.byref(bc),
+                                   None if settings is None else C.byref(settings),
+                                   C.byref(handle)))
+        return cls(handle, mesh)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.cfd_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_turbulence_model(self, model: int) -> None:
+        _check(_lib.cfd_gpu_set_turbulence(self._h, model))
+
+    def initialise(self, u, v, p, rho, mu) -> None:
+        arrays = [_f64(a) for a in (u, v, p, rho, mu)]
+        _check(_lib.cfd_gpu_initialise(self._h, *[_ptr(a) for a in arrays]))
+
+    def iterate(self, n: int = 1, history: bool = False):
+        last = Monitor()
+        hist = (Monitor * n)() if history else None
+        _check(_lib.cfd_gpu_iterate(self._h, n, C.byref(last), hist))
+        if history:
+            return last, np.stack([h.as_array() for h in hist])
+        return last
+
+    def converge(self, cap: int, tol: float):
+        last = Monitor()
+        taken = C.c_int()
+        _check(_lib.cfd_gpu_converge(self._h, cap, tol, C.byref(taken), C.byref(last)))
+        return taken.value, last
+
+    def iterate_partial(self, stage: str | int) -> Monitor:
+        last = Monitor()
+        code = STAGE[stage] if isinstance(stage, str) else stage
+        _check(_lib.cfd_gpu_iterate_partial(self._h, code, C.byref(last)))
+        return last
+
+    def read(self, name: str) -> np.ndarray:
+        n = self.mesh.cells
+        size = self.mesh.faces if name in FACE_FIELDS else (2 * n if name in VEC2_FIELDS else n)
+        out = np.zeros(size)
+        _check(_lib.cfd_gpu_read_field(self._h, FIELD[name], _ptr(out)))
+        return out
+
+    def load_state(self, u=None, v=None, p=None, mass_flux=None, k=None, omega=None, mut=None,
+                   mu_eff=None) -> None:
+        arrays = [None if a is None else _f64(a) for a in (u, v, p, mass_flux, k, omega, mut, mu_eff)]
+        _check(_lib.cfd_gpu_load_state(self._h, *[_ptr(a) for a in arrays]))
+
+    def set_settings(self, settings: Settings) -> None:
+        _check(_lib.cfd_gpu_set_settings(self._h, C.byref(settings)))
+
+    def scalars(self) -> np.ndarray:
+        out = np.zeros(3)
+        _check(_lib.cfd_gpu_scalars(self._h, _ptr(out)))
+        return out
+
+    # reference-style accessors
+    def field(self) -> dict:
+        return {name.lower(): self.read(name) for name in ("U", "V", "P", "RHO", "MU_EFF")}
+
+    def mass_flux(self) -> np.ndarray:
+        return self.read("MASS_FLUX")
+
+    def divergence(self) -> np.ndarray:
+        return self.read("DIVERGENCE")
+
+
+def library_symbols() -> list[str]:
+    """Names the C headers declare (for the ABI export check)."""
+    return [name for name in dir(_lib) if name.startswith("cfd_")]

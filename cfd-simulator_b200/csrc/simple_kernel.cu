@@ -1,0 +1,1137 @@
+// simple_kernel.cu - the SIMPLE outer iteration (laminar and k-omega SST) as
+// one persistent kernel per launch, one thread-block cluster per solve.
+//
+// Why a cluster per solve
+// -----------------------
+// A SIMPLE iteration is ~15 dependent phases, and the pressure CG inside it
+// adds two more per CG iteration (up to 200). Each phase is a 5-point stencil
+// or a reduction over 1e4-1e5 cells: far too little work to hide a kernel
+// launch or a grid-wide software barrier. A thread-block cluster gives the
+// CTAs of one solve a hardware barrier (barrier.cluster) with release/acquire
+// semantics, and distributed shared memory to exchange reduction partials,
+// so a phase boundary costs a fraction of a microsecond and no spin loop.
+// Independent solves occupy independent clusters; a batch of uneven solves is
+// a longer grid, one instance descriptor per cluster.
+//
+// Arithmetic
+// ----------
+// The plain FP64 form is built with contraction off (no FMA) and evaluates
+// every per-cell and per-face expression with the operands, association and
+// accumulation order the reference uses, so each non-reduction stage gives
+// the reference's values to the last bit. Face quantities are recomputed by
+// every cell that touches the face (the owner and the neighbour compute the
+// identical value) instead of being scattered, so no atomics are needed and
+// a cell's sums are accumulated in the reference's face order:
+//   Green-Gauss, assembly, net flux, divergence: S, N, W, E
+//     (j-faces before i-faces, ascending index; Mesh.cpp:138-170)
+//   Gauss-Seidel off-diagonal sum:               S, E, N, W
+//     (Mesh::cellFaces order, Mesh.cpp:172-181; LinearSystem.cpp:94-112)
+// Reductions (residual norms, CG dots, maxima) are deterministic: fixed-order
+// warp trees, then rank order across the cluster; every CTA derives the same
+// bits, so control flow that depends on them (CG exit, convergence) is
+// uniform. Gauss-Seidel is red-black instead of lexicographic: exact with the
+// wake cut because cellsI is even on a C-grid, so partners across the cut have
+// opposite colours. It changes the iterate path but not the converged answer.
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+
+#include <string>
+
+#include "common.hpp"
+#include "instance.hpp"
+#include "solver.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace cfdb {
+namespace {
+
+#define DEV __device__ __forceinline__
+
+// std::max / std::min / std::clamp semantics, NaN behaviour included.
+DEV double smax(double a, double b) { return (a < b) ? b : a; }
+DEV double smin(double a, double b) { return (b < a) ? b : a; }
+DEV double sclamp(double v, double lo, double hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }
+
+constexpr double kTinySolver = 1e-300;  // SimpleSolver.cpp:16
+constexpr double kTinySst = 1.0e-30;    // KOmegaSST.cpp:22
+constexpr double kMinOmega = 1.0e-10;   // KOmegaSST.cpp:20
+// SSTConstants (KOmegaSST.hpp:147-171)
+constexpr double kSigmaK1 = 0.85, kSigmaW1 = 0.5, kBeta1 = 0.075;
+constexpr double kSigmaK2 = 1.0, kSigmaW2 = 0.856, kBeta2 = 0.0828;
+constexpr double kBetaStar = 0.09, kKappa = 0.41, kA1 = 0.31, kProdLimit = 10.0;
+
+// BoundaryKind values (cfd_gpu.h).
+constexpr int kInternal = 0, kInlet = 1, kOutlet = 2, kFarField = 3, kWall = 4;
+
+constexpr int kMaxWarps = 32;
+constexpr int kRedSlots = 8;
+
+struct Shared {
+  double warp[kMaxWarps][kRedSlots];
+  double part[2][kRedSlots];
+  double result[kRedSlots];
+};
+
+struct Team {
+  cg::cluster_group cl;
+  unsigned rank, R;
+  int tid, T;
+  int c0, c1;
+  int buf;
+};
+
+// ---- reductions -------------------------------------------------------------
+
+enum RedOp : int { kSum = 0, kMax = 1 };
+
+DEV double combine(int op, double a, double b) { return (op == kMax) ? smax(a, b) : a + b; }
+DEV double identity(int op) { return (op == kMax) ? -INFINITY : 0.0; }
+
+/// Reduce K values over every thread of the cluster. The result is the same
+/// bits in every thread of every CTA. Contains a cluster barrier.
+template <int K>
+DEV void teamReduce(Team& t, Shared& sh, double (&v)[K], const int (&op)[K]) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = (t.T + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      v[k] = combine(op[k], v[k], __shfl_down_sync(0xffffffffu, v[k], off));
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) sh.warp[warp][k] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = (lane < nwarps) ? sh.warp[lane][k] : identity(op[k]);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
+      if (lane == 0) sh.part[t.buf][k] = a;
+    }
+  }
+  t.cl.sync();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = identity(op[k]);
+      if (lane < static_cast<int>(t.R)) {
+        const double* remote = t.cl.map_shared_rank(&sh.part[t.buf][k], lane);
+        a = *remote;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
+      if (lane == 0) sh.result[k] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = sh.result[k];
+  t.buf ^= 1;
+}
+
+// ---- faces of a cell ----------------------------------------------------------
+
+struct Face {
+  int fam;     // 0 N-face, 1 E-face
+  int idx;     // index within its family
+  int owner;   // owning cell
+  int nb;      // neighbour cell of an interior face, else -1
+  int other;   // nb, or the cell across the wake cut, else -1
+  bool mine;   // the cell being processed owns this face
+};
+
+DEV Face faceS(const Instance& I, int c, int i, int j) {
+  Face f;
+  f.fam = 0;
+  f.idx = j * I.NI + i;
+  if (j > 0) {
+    f.owner = c - I.NI; f.nb = c; f.other = c; f.mine = false;
+  } else {
+    f.owner = c; f.nb = -1; f.other = I.acrossJ0[i]; f.mine = true;
+  }
+  return f;
+}
+DEV Face faceN(const Instance& I, int c, int i, int j) {
+  Face f;
+  f.fam = 0;
+  f.idx = (j + 1) * I.NI + i;
+  f.owner = c;
+  f.mine = true;
+  f.nb = (j < I.NJ - 1) ? c + I.NI : -1;
+  f.other = f.nb;
+  return f;
+}
+DEV Face faceW(const Instance& I, int c, int i, int j) {
+  Face f;
+  f.fam = 1;
+  f.idx = j * (I.NI + 1) + i;
+  if (i > 0) {
+    f.owner = c - 1; f.nb = c; f.mine = false;
+  } else {
+    f.owner = c; f.nb = -1; f.mine = true;
+  }
+  f.other = f.nb;
+  return f;
+}
+DEV Face faceE(const Instance& I, int c, int i, int j) {
+  Face f;
+  f.fam = 1;
+  f.idx = j * (I.NI + 1) + i + 1;
+  f.owner = c;
+  f.mine = true;
+  f.nb = (i < I.NI - 1) ? c + 1 : -1;
+  f.other = f.nb;
+  return f;
+}
+
+DEV const FaceGeo& geo(const Instance& I, const Face& f) { return f.fam ? I.gE : I.gN; }
+DEV double massFlux(const Instance& I, const Face& f) { return f.fam ? I.mfE[f.idx] : I.mfN[f.idx]; }
+DEV double* massFluxPtr(const Instance& I, const Face& f) { return f.fam ? I.mfE + f.idx : I.mfN + f.idx; }
+DEV int kindOf(const Instance& I, const Face& f) { return f.fam ? I.kindE[f.idx] : I.kindN[f.idx]; }
+DEV double bcU(const Instance& I, const Face& f) { return f.fam ? I.bcuE[f.idx] : I.bcuN[f.idx]; }
+DEV double bcV(const Instance& I, const Face& f) { return f.fam ? I.bcvE[f.idx] : I.bcvN[f.idx]; }
+DEV double bcP(const Instance& I, const Face& f) { return f.fam ? I.bcpE[f.idx] : I.bcpN[f.idx]; }
+
+/// SimpleSolver::imposesVelocity (SimpleSolver.cpp:247-262) for a boundary face.
+DEV bool imposesVelocity(const Instance& I, const Face& f) {
+  const int kind = kindOf(I, f);
+  if (kind == kWall || kind == kInlet) return true;
+  if (kind == kFarField) {
+    const double dead = f.fam ? I.deadE[f.idx] : I.deadN[f.idx];
+    return massFlux(I, f) < dead;
+  }
+  return false;
+}
+
+/// Accumulate a face's Green-Gauss contribution S*phi into the cell's sum:
+/// added for the owner, subtracted for the neighbour (Gradient.cpp:29-40).
+DEV void ggAdd(const Face& f, double Sx, double Sy, double phi, double& gx, double& gy) {
+  const double cx = Sx * phi, cy = Sy * phi;
+  if (f.mine) {
+    gx += cx; gy += cy;
+  } else {
+    gx -= cx; gy -= cy;
+  }
+}
+
+DEV void ggFinish(double vol, double& gx, double& gy) {
+  if (vol > 0.0) {
+    const double s = 1.0 / vol;
+    gx *= s;
+    gy *= s;
+  }
+}
+
+/// Cell on the other side of face k (0 S, 1 N, 2 W, 3 E) of cell (i, j), or -1.
+DEV int across(const Instance& I, int c, int i, int j, int k) {
+  switch (k) {
+    case 0: return (j > 0) ? c - I.NI : I.acrossJ0[i];
+    case 1: return (j < I.NJ - 1) ? c + I.NI : -1;
+    case 2: return (i > 0) ? c - 1 : -1;
+    default: return (i < I.NI - 1) ? c + 1 : -1;
+  }
+}
+
+// ---- phase: face values + Green-Gauss gradients of u, v, p ---------------------
+
+/// interpolateFaceValues (SimpleSolver.cpp:268-304) for one face.
+DEV void faceUVP(const Instance& I, const Face& f, double& fu, double& fv, double& fp) {
+  const int o = f.owner;
+  if (f.other >= 0) {
+    const double w = geo(I, f).w[f.idx];
+    const int n = f.other;
+    fu = w * I.u[o] + (1.0 - w) * I.u[n];
+    fv = w * I.v[o] + (1.0 - w) * I.v[n];
+    fp = w * I.p[o] + (1.0 - w) * I.p[n];
+    return;
+  }
+  if (imposesVelocity(I, f)) {
+    fu = bcU(I, f);
+    fv = bcV(I, f);
+    fp = I.p[o];
+  } else {
+    fu = I.u[o];
+    fv = I.v[o];
+    fp = bcP(I, f);
+  }
+}
+
+DEV void phaseGradients(const Instance& I, Team& t, double& speedMax) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double ux = 0.0, uy = 0.0, vx = 0.0, vy = 0.0, px = 0.0, py = 0.0;
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      double fu, fv, fp;
+      faceUVP(I, f, fu, fv, fp);
+      const FaceGeo& g = geo(I, f);
+      const double Sx = g.Sx[f.idx], Sy = g.Sy[f.idx];
+      ggAdd(f, Sx, Sy, fu, ux, uy);
+      ggAdd(f, Sx, Sy, fv, vx, vy);
+      ggAdd(f, Sx, Sy, fp, px, py);
+    }
+    const double vol = I.vol[c];
+    ggFinish(vol, ux, uy);
+    ggFinish(vol, vx, vy);
+    ggFinish(vol, px, py);
+    I.gux[c] = ux; I.guy[c] = uy;
+    I.gvx[c] = vx; I.gvy[c] = vy;
+    I.gpx[c] = px; I.gpy[c] = py;
+    speedMax = smax(speedMax, hypot(I.u[c], I.v[c]));
+  }
+}
+
+// ---- phase: momentum assembly (u and v share the matrix), relaxation, residual --
+
+DEV void phaseMomentum(const Instance& I, Team& t, double& resU, double& resV, double& diagL1) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double diag = 0.0, sU = 0.0, sV = 0.0;
+    double off[4] = {0.0, 0.0, 0.0, 0.0};  // coefficient on the S, N, W, E cell
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      const FaceGeo& g = geo(I, f);
+      const int o = f.owner;
+      const double flux = massFlux(I, f);
+      if (f.other >= 0) {
+        const int n = f.other;
+        const double w = g.w[f.idx];
+        const double vis = w * I.mu[o] + (1.0 - w) * I.mu[n];
+        const double dif = vis * g.D[f.idx];
+        const double outward = smax(flux, 0.0);
+        const double inward = smax(-flux, 0.0);
+        const double Tx = g.Tx[f.idx], Ty = g.Ty[f.idx];
+        const double fgux = I.gux[o] * w + I.gux[n] * (1.0 - w);
+        const double fguy = I.guy[o] * w + I.guy[n] * (1.0 - w);
+        const double fgvx = I.gvx[o] * w + I.gvx[n] * (1.0 - w);
+        const double fgvy = I.gvy[o] * w + I.gvy[n] * (1.0 - w);
+        const double cu = I.blend * vis * (fgux * Tx + fguy * Ty);
+        const double cv = I.blend * vis * (fgvx * Tx + fgvy * Ty);
+        if (f.nb >= 0) {
+          double du = 0.0, dv = 0.0;
+          if (I.sou) {
+            const double uo = I.u[o], un = I.u[n], vo = I.v[o], vn = I.v[n];
+            du = flux * ((w * uo + (1.0 - w) * un) - ((flux >= 0.0) ? uo : un));
+            dv = flux * ((w * vo + (1.0 - w) * vn) - ((flux >= 0.0) ? vo : vn));
+          }
+          if (f.mine) {
+            diag += outward + dif;
+            off[k] = 0.0 + (-inward - dif);
+            sU += cu; sV += cv;
+            if (I.sou) { sU -= du; sV -= dv; }
+          } else {
+            diag += inward + dif;
+            off[k] = 0.0 + (-outward - dif);
+            sU -= cu; sV -= cv;
+            if (I.sou) { sU += du; sV += dv; }
+          }
+        } else {
+          // Wake cut: the owner's row only (SimpleSolver.cpp:379-398).
+          diag += outward + dif;
+          off[k] = 0.0 + (-inward - dif);
+          sU += cu; sV += cv;
+        }
+        continue;
+      }
+      // Boundary face (SimpleSolver.cpp:400-416).
+      const double vis = I.mu[o];
+      const double dif = vis * g.D[f.idx];
+      if (imposesVelocity(I, f)) {
+        const double iu = bcU(I, f), iv = bcV(I, f);
+        const double Tx = g.Tx[f.idx], Ty = g.Ty[f.idx];
+        sU -= flux * iu; sV -= flux * iv;
+        diag += dif;
+        sU += dif * iu; sV += dif * iv;
+        sU += I.blend * vis * (I.gux[o] * Tx + I.guy[o] * Ty);
+        sV += I.blend * vis * (I.gvx[o] * Tx + I.gvy[o] * Ty);
+      } else {
+        diag += flux;
+      }
+    }
+    const double vol = I.vol[c];
+    sU -= I.gpx[c] * vol;
+    sV -= I.gpy[c] * vol;
+    // applyRelaxation (SimpleSolver.cpp:425-443).
+    const double uc = I.u[c], vc = I.v[c];
+    if (!(fabs(diag) > 0.0)) {
+      diag = 1.0;
+    } else {
+      const double relaxed = diag / I.alphaU;
+      sU += (relaxed - diag) * uc;
+      sV += (relaxed - diag) * vc;
+      diag = relaxed;
+    }
+    I.aD[c] = diag; I.aS[c] = off[0]; I.aN[c] = off[1]; I.aW[c] = off[2]; I.aE[c] = off[3];
+    I.bU[c] = sU; I.bV[c] = sV;
+    // residualL1 (LinearSystem.cpp:45-54): y = A x in multiply's face order.
+    double yu = diag * uc, yv = diag * vc;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int n = across(I, c, i, j, k);
+      if (n >= 0) {
+        yu += off[k] * I.u[n];
+        yv += off[k] * I.v[n];
+      }
+    }
+    resU += fabs(sU - yu);
+    resV += fabs(sV - yv);
+    diagL1 += fabs(diag);
+  }
+}
+
+/// One red-black Gauss-Seidel colour pass on one or two systems sharing the
+/// cell order (LinearSystem.cpp:77-116, off-diagonals summed S, E, N, W).
+DEV void gsColour(const Instance& I, Team& t, int colour, const double* D, const double* cS,
+                  const double* cN, const double* cW, const double* cE, const double* b1, double* x1,
+                  const double* D2, const double* cS2, const double* cN2, const double* cW2,
+                  const double* cE2, const double* b2, double* x2) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    if (((i + j) & 1) != colour) continue;
+    const int nS = across(I, c, i, j, 0), nN = across(I, c, i, j, 1);
+    const int nW = across(I, c, i, j, 2), nE = across(I, c, i, j, 3);
+    {
+      const double d = D[c];
+      if (fabs(d) > 0.0) {
+        double off = 0.0;
+        if (nS >= 0) off += cS[c] * x1[nS];
+        if (nE >= 0) off += cE[c] * x1[nE];
+        if (nN >= 0) off += cN[c] * x1[nN];
+        if (nW >= 0) off += cW[c] * x1[nW];
+        x1[c] = (b1[c] - off) / d;
+      }
+    }
+    if (x2 != nullptr) {
+      const double d = D2[c];
+      if (fabs(d) > 0.0) {
+        double off = 0.0;
+        if (nS >= 0) off += cS2[c] * x2[nS];
+        if (nE >= 0) off += cE2[c] * x2[nE];
+        if (nN >= 0) off += cN2[c] * x2[nN];
+        if (nW >= 0) off += cW2[c] * x2[nW];
+        x2[c] = (b2[c] - off) / d;
+      }
+    }
+  }
+}
+
+// ---- phase: Rhie-Chow face fluxes (SimpleSolver.cpp:445-496) -------------------
+
+DEV void rhieChowFace(const Instance& I, const Face& f) {
+  const FaceGeo& g = geo(I, f);
+  const int o = f.owner;
+  const double Sx = g.Sx[f.idx], Sy = g.Sy[f.idx], D = g.D[f.idx];
+  double* mf = massFluxPtr(I, f);
+  if (f.other >= 0) {
+    const int n = f.other;
+    const double w = g.w[f.idx];
+    const double ix = I.u[o] * w + I.u[n] * (1.0 - w);
+    const double iy = I.v[o] * w + I.v[n] * (1.0 - w);
+    const double dens = w * I.rho[o] + (1.0 - w) * I.rho[n];
+    const double mob = w * (I.vol[o] / I.aD[o]) + (1.0 - w) * (I.vol[n] / I.aD[n]);
+    const double sgx = I.gpx[o] * w + I.gpx[n] * (1.0 - w);
+    const double sgy = I.gpy[o] * w + I.gpy[n] * (1.0 - w);
+    const double compact = (I.p[n] - I.p[o]) * D;
+    const double smooth = sgx * Sx + sgy * Sy;
+    *mf = dens * (ix * Sx + iy * Sy) - dens * mob * (compact - smooth);
+    return;
+  }
+  const double dens = I.rho[o];
+  if (imposesVelocity(I, f)) {
+    *mf = dens * (bcU(I, f) * Sx + bcV(I, f) * Sy);
+  } else {
+    const double mob = I.vol[o] / I.aD[o];
+    const double compact = (bcP(I, f) - I.p[o]) * D;
+    const double smooth = I.gpx[o] * Sx + I.gpy[o] * Sy;
+    *mf = dens * (I.u[o] * Sx + I.v[o] * Sy) - dens * mob * (compact - smooth);
+  }
+}
+
+DEV void phaseRhieChow(const Instance& I, Team& t) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    if (j == 0) rhieChowFace(I, faceS(I, c, i, j));
+    rhieChowFace(I, faceN(I, c, i, j));
+    if (i == 0) rhieChowFace(I, faceW(I, c, i, j));
+    rhieChowFace(I, faceE(I, c, i, j));
+  }
+}
+
+// ---- phase: pressure-correction assembly (SimpleSolver.cpp:498-580) ------------
+
+/// rho_f * mobility_f * D for a face with a cell on each side (the same
+/// coefficient the flux correction uses).
+DEV double pressureCoefficient(const Instance& I, const Face& f, int n) {
+  const FaceGeo& g = geo(I, f);
+  const int o = f.owner;
+  const double w = g.w[f.idx];
+  const double dens = w * I.rho[o] + (1.0 - w) * I.rho[n];
+  const double mob = w * (I.vol[o] / I.aD[o]) + (1.0 - w) * (I.vol[n] / I.aD[n]);
+  return dens * mob * g.D[f.idx];
+}
+
+DEV void phasePressureAssembly(const Instance& I, Team& t, double& netL1, double& bSum) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double net = 0.0, diag = 0.0;
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      const double flux = massFlux(I, f);
+      if (f.mine) net += flux; else net -= flux;
+      if (f.other >= 0) {
+        const double coef = pressureCoefficient(I, f, f.other);
+        diag += coef;
+        if (f.mine) {
+          double* slot = f.fam ? I.pE + f.idx : I.pN + f.idx;
+          *slot = 0.0 + (-coef);
+        }
+        continue;
+      }
+      if (imposesVelocity(I, f)) continue;
+      const double mob = I.vol[c] / I.aD[c];
+      diag += I.rho[c] * mob * geo(I, f).D[f.idx];
+    }
+    I.net[c] = net;
+    I.pD[c] = diag;
+    I.pB[c] = -net;
+    netL1 += fabs(net);
+    bSum += -net;
+  }
+}
+
+/// y = A x for the pressure-correction matrix, in multiply's face order.
+DEV double pressureRow(const Instance& I, int c, int i, int j, const double* xv, double xc) {
+  double y = I.pD[c] * xc;
+  if (j > 0) y += I.pN[j * I.NI + i] * xv[c - I.NI];
+  else if (I.acrossJ0[i] >= 0) y += I.pN[i] * xv[I.acrossJ0[i]];
+  if (j < I.NJ - 1) y += I.pN[(j + 1) * I.NI + i] * xv[c + I.NI];
+  if (i > 0) y += I.pE[j * (I.NI + 1) + i] * xv[c - 1];
+  if (i < I.NI - 1) y += I.pE[j * (I.NI + 1) + i + 1] * xv[c + 1];
+  return y;
+}
+
+// ---- phase: correction (SimpleSolver.cpp:582-660) ------------------------------
+
+DEV void correctFace(const Instance& I, const Face& f) {
+  const FaceGeo& g = geo(I, f);
+  const int o = f.owner;
+  double* mf = massFluxPtr(I, f);
+  if (f.other >= 0) {
+    const int n = f.other;
+    const double w = g.w[f.idx];
+    const double dens = w * I.rho[o] + (1.0 - w) * I.rho[n];
+    const double mob = w * (I.vol[o] / I.aD[o]) + (1.0 - w) * (I.vol[n] / I.aD[n]);
+    *mf -= dens * mob * g.D[f.idx] * (I.x[n] - I.x[o]);
+    return;
+  }
+  if (imposesVelocity(I, f)) return;
+  const double mob = I.vol[o] / I.aD[o];
+  *mf -= I.rho[o] * mob * g.D[f.idx] * (0.0 - I.x[o]);
+}
+
+DEV void phaseCorrect(const Instance& I, Team& t) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double gx = 0.0, gy = 0.0;
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      const FaceGeo& g = geo(I, f);
+      double fc;
+      if (f.other >= 0) {
+        const double w = g.w[f.idx];
+        fc = w * I.x[f.owner] + (1.0 - w) * I.x[f.other];
+      } else if (imposesVelocity(I, f)) {
+        fc = I.x[f.owner];
+      } else {
+        fc = 0.0;
+      }
+      ggAdd(f, g.Sx[f.idx], g.Sy[f.idx], fc, gx, gy);
+    }
+    ggFinish(I.vol[c], gx, gy);
+    I.p[c] += I.alphaP * I.x[c];
+    const double mob = I.vol[c] / I.aD[c];
+    I.u[c] -= gx * mob;
+    I.v[c] -= gy * mob;
+    if (j == 0) correctFace(I, fs[0]);
+    correctFace(I, fs[1]);
+    if (i == 0) correctFace(I, fs[2]);
+    correctFace(I, fs[3]);
+  }
+}
+
+// ---- divergence (SimpleSolver.cpp:796-817) -------------------------------------
+
+DEV double cellDivergence(const Instance& I, int c, int i, int j) {
+  double net = 0.0;
+  const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const Face& f = fs[k];
+    const double dens = smax(I.rho[f.owner], kTinySolver);
+    const double vf = massFlux(I, f) / dens;
+    if (f.mine) net += vf; else net -= vf;
+  }
+  const double area = I.vol[c];
+  return (area > 0.0) ? net / area : 0.0;
+}
+
+// ---- k-omega SST (KOmegaSST.cpp) -----------------------------------------------
+
+/// Face value of k or omega (KOmegaSST.cpp:26-68, with the no-slip override
+/// of :236-241 for omega). isOmega selects the wall treatment.
+DEV double sstFaceValue(const Instance& I, const Face& f, const double* phi, bool isOmega) {
+  const int o = f.owner;
+  if (f.nb >= 0) {
+    const double w = geo(I, f).w[f.idx];
+    return w * phi[o] + (1.0 - w) * phi[f.nb];
+  }
+  if (f.other >= 0) {
+    const double w = 1.0;  // ownerWeight() of a face without a neighbour
+    return w * phi[o] + (1.0 - w) * phi[f.other];
+  }
+  const double inflow = isOmega ? I.wIn : I.kIn;
+  switch (kindOf(I, f)) {
+    case kWall: return isOmega ? phi[o] : 0.0;
+    case kInlet: return inflow;
+    case kFarField: return (massFlux(I, f) < 0.0) ? inflow : phi[o];
+    default: return phi[o];
+  }
+}
+
+DEV void phaseSstBlending(const Instance& I, Team& t, double& divMax) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    divMax = smax(divMax, fabs(cellDivergence(I, c, i, j)));
+    // computeStrain (:202-216), gradients from the start of the iteration.
+    const double s11 = I.gux[c], s22 = I.gvy[c];
+    const double s12 = 0.5 * (I.guy[c] + I.gvx[c]);
+    const double S = sqrt(2.0 * (s11 * s11 + s22 * s22 + 2.0 * s12 * s12));
+    I.strain[c] = S;
+    // Green-Gauss gradients of k and omega (:224-244).
+    double kx = 0.0, ky = 0.0, wx = 0.0, wy = 0.0;
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      const FaceGeo& g = geo(I, f);
+      const double Sx = g.Sx[f.idx], Sy = g.Sy[f.idx];
+      ggAdd(f, Sx, Sy, sstFaceValue(I, f, I.k, false), kx, ky);
+      ggAdd(f, Sx, Sy, sstFaceValue(I, f, I.om, true), wx, wy);
+    }
+    const double vol = I.vol[c];
+    ggFinish(vol, kx, ky);
+    ggFinish(vol, wx, wy);
+    I.gkx[c] = kx; I.gky[c] = ky; I.gwx[c] = wx; I.gwy[c] = wy;
+    // Cross-diffusion and the blending functions (:247-286).
+    const double d = smax(I.wallDist[c], kTinySst);
+    const double rho = I.rho[c];
+    const double nu = I.muMol[c] / smax(rho, kTinySst);
+    const double omega = smax(I.om[c], kMinOmega);
+    const double energy = smax(I.k[c], 0.0);
+    const double cdv = 2.0 * rho * kSigmaW2 * (kx * wx + ky * wy) / omega;
+    const double cdp = smax(cdv, 1.0e-10);
+    const double term1 = sqrt(smax(energy, 0.0)) / (kBetaStar * omega * d);
+    const double term2 = 500.0 * nu / (d * d * omega);
+    const double term3 = 4.0 * rho * kSigmaW2 * energy / (cdp * d * d);
+    const double arg1 = smin(smax(term1, term2), term3);
+    const double F1 = tanh(sclamp(arg1 * arg1 * arg1 * arg1, 0.0, 50.0));
+    const double arg2 = smax(2.0 * term1, term2);
+    const double F2 = tanh(sclamp(arg2 * arg2, 0.0, 50.0));
+    I.cd[c] = cdv;
+    I.f1[c] = F1;
+    I.f2[c] = F2;
+    // Limited production (:362-368).
+    const double raw = I.mut[c] * S * S;
+    const double ceiling = kProdLimit * kBetaStar * rho * smax(I.k[c], 0.0) * smax(I.om[c], kMinOmega);
+    I.prod[c] = smin(raw, ceiling);
+  }
+}
+
+DEV double blendF1(double f1, double nearValue, double farValue) { return f1 * nearValue + (1.0 - f1) * farValue; }
+
+/// Assemble, relax and measure one row of the k and of the omega equation
+/// (KOmegaSST.cpp:378-466); both equations in one pass over the faces.
+DEV void phaseSstAssembly(const Instance& I, Team& t, double (&acc)[4]) {
+  const double relax = sclamp(I.alphaT, 0.05, 1.0);
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double dK = 0.0, bK = 0.0, dW = 0.0, bW = 0.0;
+    double oK[4] = {0.0, 0.0, 0.0, 0.0}, oW[4] = {0.0, 0.0, 0.0, 0.0};
+    const Face fs[4] = {faceS(I, c, i, j), faceN(I, c, i, j), faceW(I, c, i, j), faceE(I, c, i, j)};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const Face& f = fs[k];
+      const FaceGeo& g = geo(I, f);
+      const int o = f.owner;
+      const double flux = massFlux(I, f);
+      const double Dt = g.Dt[f.idx];
+      if (f.other >= 0) {
+        const int n = f.other;
+        const double w = (f.nb >= 0) ? g.w[f.idx] : 1.0;
+        const double f1o = I.f1[o], f1n = I.f1[n];
+        const double sko = blendF1(f1o, kSigmaK1, kSigmaK2), skn = blendF1(f1n, kSigmaK1, kSigmaK2);
+        const double swo = blendF1(f1o, kSigmaW1, kSigmaW2), swn = blendF1(f1n, kSigmaW1, kSigmaW2);
+        const double muo = I.muMol[o], mun = I.muMol[n], mto = I.mut[o], mtn = I.mut[n];
+        const double difK = (w * (muo + sko * mto) + (1.0 - w) * (mun + skn * mtn)) * Dt;
+        const double difW = (w * (muo + swo * mto) + (1.0 - w) * (mun + swn * mtn)) * Dt;
+        const double outward = smax(flux, 0.0);
+        const double inward = smax(-flux, 0.0);
+        if (f.mine) {
+          dK += outward + difK;
+          dW += outward + difW;
+          oK[k] = 0.0 + (-inward - difK);
+          oW[k] = 0.0 + (-inward - difW);
+        } else {
+          dK += inward + difK;
+          dW += inward + difW;
+          oK[k] = 0.0 + (-outward - difK);
+          oW[k] = 0.0 + (-outward - difW);
+        }
+        continue;
+      }
+      const double f1o = I.f1[o];
+      const double difK = (I.muMol[o] + blendF1(f1o, kSigmaK1, kSigmaK2) * I.mut[o]) * Dt;
+      const double difW = (I.muMol[o] + blendF1(f1o, kSigmaW1, kSigmaW2) * I.mut[o]) * Dt;
+      const int kind = kindOf(I, f);
+      const bool imposed = kind == kWall || kind == kInlet || (kind == kFarField && flux < 0.0);
+      if (imposed) {
+        const double valK = (kind == kWall) ? 0.0 : I.kIn;
+        const double valW = I.wIn;  // the omega equation's wall value is its inflow value
+        dK += difK + smax(flux, 0.0);
+        bK += (difK - smin(flux, 0.0)) * valK;
+        dW += difW + smax(flux, 0.0);
+        bW += (difW - smin(flux, 0.0)) * valW;
+      } else {
+        dK += smax(flux, 0.0);
+        dW += smax(flux, 0.0);
+      }
+    }
+    // Sources (:446-453): explicit production, implicit destruction.
+    const double vol = I.vol[c];
+    const double rho = I.rho[c];
+    const double F1 = I.f1[c];
+    const double omPos = smax(I.om[c], kMinOmega);
+    const double S = I.strain[c];
+    bK += I.prod[c] * vol;
+    dK += kBetaStar * rho * omPos * vol;
+    const double gamma = blendF1(F1, I.gamma1, I.gamma2);
+    const double beta = blendF1(F1, kBeta1, kBeta2);
+    double wProd = gamma * rho * S * S;
+    wProd += (1.0 - F1) * I.cd[c];
+    bW += wProd * vol;
+    dW += beta * rho * omPos * vol;
+    // Implicit under-relaxation (:455-463).
+    const double kc = I.k[c], wc = I.om[c];
+    if (fabs(dK) > kTinySst) {
+      const double relaxed = dK / relax;
+      bK += (relaxed - dK) * kc;
+      dK = relaxed;
+    }
+    if (fabs(dW) > kTinySst) {
+      const double relaxed = dW / relax;
+      bW += (relaxed - dW) * wc;
+      dW = relaxed;
+    }
+    I.kD[c] = dK; I.kS[c] = oK[0]; I.kN[c] = oK[1]; I.kW[c] = oK[2]; I.kE[c] = oK[3]; I.kB[c] = bK;
+    I.wD[c] = dW; I.wS[c] = oW[0]; I.wN[c] = oW[1]; I.wW[c] = oW[2]; I.wE[c] = oW[3]; I.wB[c] = bW;
+    double yk = dK * kc, yw = dW * wc;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int n = across(I, c, i, j, k);
+      if (n >= 0) {
+        yk += oK[k] * I.k[n];
+        yw += oW[k] * I.om[n];
+      }
+    }
+    acc[0] += fabs(bK - yk);
+    acc[1] += fabs(dK);
+    acc[2] += fabs(bW - yw);
+    acc[3] += fabs(dW);
+  }
+}
+
+/// wallOmega (KOmegaSST.cpp:86-92).
+DEV double wallOmega(const Instance& I, double nu, double distance, double energy) {
+  const double d = smax(distance, kTinySst);
+  const double viscous = 6.0 * nu / (kBeta1 * d * d);
+  const double logarithmic = sqrt(smax(energy, 0.0)) / (I.betaStarQuarter * kKappa * d);
+  return sqrt(viscous * viscous + logarithmic * logarithmic);
+}
+
+/// Floors, wall conditions, eddy viscosity, ranges (KOmegaSST.cpp:289-345,
+/// :469-471, :513-529; SimpleSolver.cpp:232-245, :782-790).
+DEV void phaseSstFinish(const Instance& I, Team& t, double (&mx)[8]) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    double kc = smax(I.k[c], 0.0);
+    double wc = smax(I.om[c], kMinOmega);
+    const uint8_t mask = I.wallMask[c];
+    if (mask != 0) {
+      const double d = smax(I.wallDist[c], kTinySst);
+      const double rho = smax(I.rho[c], kTinySst);
+      const double mu = I.muMol[c];
+      const double nu = mu / rho;
+      wc = wallOmega(I, nu, d, kc);
+      const double uc = I.u[c], vc = I.v[c];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (!(mask & (1u << k))) continue;
+        const Face f = (k == 0) ? faceS(I, c, i, j) : (k == 1) ? faceN(I, c, i, j)
+                                 : (k == 2) ? faceW(I, c, i, j) : faceE(I, c, i, j);
+        const FaceGeo& g = geo(I, f);
+        const double nX = g.nx[f.idx] * -1.0, nY = g.ny[f.idx] * -1.0;
+        const double dn = uc * nX + vc * nY;
+        const double px = uc - nX * dn, py = vc - nY * dn;
+        const double tangential = hypot(px, py);
+        const double shear = mu * tangential / d;
+        const double fv = sqrt(shear / rho);
+        mx[5] = smax(mx[5], fv * d / smax(nu, kTinySst));
+      }
+    }
+    I.k[c] = kc;
+    I.om[c] = wc;
+    const double denom = smax(kA1 * smax(wc, kMinOmega), I.strain[c] * I.f2[c]);
+    const double mut = I.rho[c] * kA1 * smax(kc, 0.0) / smax(denom, kTinySst);
+    I.mut[c] = mut;
+    I.mu[c] = I.muMol[c] + mut;
+    // ranges: max of (k, omega, mut) and of their negatives (for the minima)
+    mx[0] = smax(mx[0], kc); mx[1] = smax(mx[1], -kc);
+    mx[2] = smax(mx[2], wc); mx[3] = smax(mx[3], -wc);
+    mx[4] = smax(mx[4], mut); mx[6] = smax(mx[6], -mut);
+    const double muMol = I.muMol[c];
+    if (muMol > 0.0) mx[7] = smax(mx[7], mut / muMol);
+  }
+}
+
+}  // namespace
+
+// ---- the kernel -----------------------------------------------------------------
+
+/// Run `iterations` outer iterations (or fewer: `stopStage` ends the first
+/// iteration early; `tolerance` >= 0 stops at convergence or divergence as
+/// SolverWorker does, SolverWorker.cpp:164-185). One cluster per instance.
+__global__ void __launch_bounds__(512, 1)
+simpleKernel(const Instance* __restrict__ instances, int iterations, int stopStage, double tolerance) {
+  __shared__ Shared sh;
+  Team t{cg::this_cluster(), 0, 0, 0, 0, 0, 0, 0};
+  t.rank = t.cl.block_rank();
+  t.R = t.cl.num_blocks();
+  t.tid = threadIdx.x;
+  t.T = blockDim.x;
+  const Instance& I = instances[blockIdx.x / t.R];
+  t.c0 = static_cast<int>((static_cast<long long>(I.N) * t.rank) / t.R);
+  t.c1 = static_cast<int>((static_cast<long long>(I.N) * (t.rank + 1)) / t.R);
+  const bool sst = (I.model == 2);
+  const bool leader = (t.rank == 0 && t.tid == 0);
+
+  int done = 0;
+  for (int it = 0; it < iterations; ++it) {
+    double mon[kMonSlots];
+#pragma unroll
+    for (int s = 0; s < kMonSlots; ++s) mon[s] = 0.0;
+
+    // 1. face values and gradients; velocity scale.
+    {
+      double v1[1] = {0.0};
+      const int op[1] = {kMax};
+      phaseGradients(I, t, v1[0]);
+      teamReduce(t, sh, v1, op);
+      double scale = smax(0.0, v1[0]);
+      if (!(scale > 0.0)) scale = 1.0;
+      mon[kMonMomX] = scale;  // held until the residuals are known
+    }
+    if (stopStage == kStageGradients) { done = it + 1; break; }
+
+    // 2. momentum assembly + relaxation + residuals (u and v together).
+    {
+      double v3[3] = {0.0, 0.0, 0.0};
+      const int op[3] = {kSum, kSum, kSum};
+      phaseMomentum(I, t, v3[0], v3[1], v3[2]);
+      teamReduce(t, sh, v3, op);
+      const double scale = v3[2] * mon[kMonMomX];
+      mon[kMonMomX] = v3[0] / smax(scale, kTinySolver);
+      mon[kMonMomY] = v3[1] / smax(scale, kTinySolver);
+    }
+    if (stopStage == kStageMomentumAssembly) { done = it + 1; break; }
+
+    // 3. Gauss-Seidel sweeps, red-black, u and v together.
+    for (int sweep = 0; sweep < I.sweeps; ++sweep) {
+      for (int colour = 0; colour < 2; ++colour) {
+        gsColour(I, t, colour, I.aD, I.aS, I.aN, I.aW, I.aE, I.bU, I.u, I.aD, I.aS, I.aN, I.aW,
+                 I.aE, I.bV, I.v);
+        t.cl.sync();
+      }
+    }
+    if (stopStage == kStageMomentumSolve) { done = it + 1; break; }
+
+    // 4. Rhie-Chow face fluxes.
+    phaseRhieChow(I, t);
+    t.cl.sync();
+    if (stopStage == kStageRhieChow) { done = it + 1; break; }
+
+    bool stopped = false;
+    const int passes = (I.nCorr > 1) ? I.nCorr : 1;
+    for (int pass = 0; pass < passes && !stopped; ++pass) {
+      // 5. pressure-correction assembly; CG start (x = 0, r = b, d = z = M^-1 r).
+      double v2[2] = {0.0, 0.0};
+      const int op2[2] = {kSum, kSum};
+      phasePressureAssembly(I, t, v2[0], v2[1]);
+      teamReduce(t, sh, v2, op2);
+      if (pass == 0) {
+        mon[kMonMassImbalance] = v2[0];
+        mon[kMonContinuity] = v2[0] / I.refMassFlow;
+      }
+      const double mean = I.hasPRef ? 0.0 : v2[1] / static_cast<double>(I.N);
+      double init[2] = {0.0, 0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        double b = I.pB[c];
+        if (!I.hasPRef) { b -= mean; I.pB[c] = b; }
+        const double dg = I.pD[c];
+        const double zc = (fabs(dg) > 0.0) ? b / dg : b;
+        I.x[c] = 0.0;
+        I.r[c] = b;
+        I.z[c] = zc;
+        I.d0[c] = zc;
+        init[0] += fabs(b);
+        init[1] += b * zc;
+      }
+      teamReduce(t, sh, init, op2);
+      if (stopStage == kStagePressureAssembly) { stopped = true; break; }
+
+      // 6. Jacobi-preconditioned CG (LinearSystem.cpp:118-210), two cluster
+      // barriers per iteration: the next direction d' = z + beta d is formed
+      // redundantly for each neighbour from z and d, which are both stable
+      // across the barrier, so A d' needs no extra exchange.
+      const double initial = init[0];
+      double rz = init[1];
+      int cgIters = 0;
+      if (initial > 0.0) {
+        double* dCur = I.d0;
+        double* dNext = I.d1;
+        double beta = 0.0;
+        for (int iter = 0; iter < I.cgMax; ++iter) {
+          double dAd[1] = {0.0};
+          const int opS[1] = {kSum};
+          for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+            const int i = c % I.NI, j = c / I.NI;
+            double dc;
+            if (iter == 0) {
+              dc = dCur[c];
+              I.q[c] = pressureRow(I, c, i, j, dCur, dc);
+            } else {
+              // d' for this cell and its neighbours, then A d'.
+              dc = I.z[c] + beta * dCur[c];
+              dNext[c] = dc;
+              double y = I.pD[c] * dc;
+              int n = (j > 0) ? c - I.NI : I.acrossJ0[i];
+              if (n >= 0) y += I.pN[j * I.NI + i] * (I.z[n] + beta * dCur[n]);
+              if (j < I.NJ - 1) { n = c + I.NI; y += I.pN[(j + 1) * I.NI + i] * (I.z[n] + beta * dCur[n]); }
+              if (i > 0) { n = c - 1; y += I.pE[j * (I.NI + 1) + i] * (I.z[n] + beta * dCur[n]); }
+              if (i < I.NI - 1) { n = c + 1; y += I.pE[j * (I.NI + 1) + i + 1] * (I.z[n] + beta * dCur[n]); }
+              I.q[c] = y;
+            }
+            dAd[0] += dc * I.q[c];
+          }
+          if (iter > 0) { double* tmp = dCur; dCur = dNext; dNext = tmp; }
+          teamReduce(t, sh, dAd, opS);
+          if (!(fabs(dAd[0]) > 0.0)) break;
+          const double step = rz / dAd[0];
+          double rr[2] = {0.0, 0.0};
+          for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+            const double dc = dCur[c];
+            I.x[c] += step * dc;
+            const double rc = I.r[c] - step * I.q[c];
+            I.r[c] = rc;
+            const double dg = I.pD[c];
+            const double zc = (fabs(dg) > 0.0) ? rc / dg : rc;
+            I.z[c] = zc;
+            rr[0] += fabs(rc);
+            rr[1] += rc * zc;
+          }
+          teamReduce(t, sh, rr, op2);
+          cgIters = iter + 1;
+          if (rr[0] <= I.cgTol * initial) break;
+          if (!(fabs(rz) > 0.0)) break;
+          beta = rr[1] / rz;
+          rz = rr[1];
+        }
+      }
+      mon[kMonPressureIterations] += static_cast<double>(cgIters);
+      if (!I.hasPRef) {
+        double sx[1] = {0.0};
+        const int opS[1] = {kSum};
+        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) sx[0] += I.x[c];
+        teamReduce(t, sh, sx, opS);
+        const double m = sx[0] / static_cast<double>(I.N);
+        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] -= m;
+        t.cl.sync();
+      }
+      if (stopStage == kStagePressureSolve) { stopped = true; break; }
+
+      // 7. correct p, u, v and the face fluxes.
+      phaseCorrect(I, t);
+      t.cl.sync();
+      if (stopStage == kStageCorrect) { stopped = true; break; }
+    }
+    if (stopped) {
+      if (leader) {
+        for (int s = 0; s < kMonSlots; ++s) I.history[it * kMonSlots + s] = mon[s];
+      }
+      done = it + 1;
+      break;
+    }
+
+    // 8. divergence (+ SST strain, gradients of k and omega, blending, production).
+    if (sst) {
+      double v1[1] = {0.0};
+      const int op[1] = {kMax};
+      phaseSstBlending(I, t, v1[0]);
+      teamReduce(t, sh, v1, op);
+      mon[kMonMaxDivergence] = smax(0.0, v1[0]);
+      if (stopStage == kStageSstBlending) { done = it + 1; break; }
+
+      double a4[4] = {0.0, 0.0, 0.0, 0.0};
+      const int op4[4] = {kSum, kSum, kSum, kSum};
+      phaseSstAssembly(I, t, a4);
+      teamReduce(t, sh, a4, op4);
+      mon[kMonTurbFirst] = a4[0] / smax(a4[1] * smax(I.kIn, kTinySst), kTinySst);
+      mon[kMonTurbSecond] = a4[2] / smax(a4[3] * smax(I.wIn, kTinySst), kTinySst);
+      if (stopStage == kStageSstAssembly) { done = it + 1; break; }
+
+      for (int sweep = 0; sweep < 3; ++sweep) {
+        for (int colour = 0; colour < 2; ++colour) {
+          gsColour(I, t, colour, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN, I.wW,
+                   I.wE, I.wB, I.om);
+          t.cl.sync();
+        }
+      }
+      if (stopStage == kStageSstSolve) { done = it + 1; break; }
+
+      double m8[8];
+#pragma unroll
+      for (int s = 0; s < 8; ++s) m8[s] = -INFINITY;
+      m8[5] = 0.0;
+      m8[7] = 0.0;
+      const int op8[8] = {kMax, kMax, kMax, kMax, kMax, kMax, kMax, kMax};
+      phaseSstFinish(I, t, m8);
+      teamReduce(t, sh, m8, op8);
+      mon[kMonMaxK] = m8[0]; mon[kMonMinK] = -m8[1];
+      mon[kMonMaxW] = m8[2]; mon[kMonMinW] = -m8[3];
+      mon[kMonMaxMut] = m8[4]; mon[kMonMinMut] = -m8[6];
+      mon[kMonMaxYPlus] = m8[5];
+      mon[kMonMaxRatio] = m8[7];
+    } else {
+      double v1[1] = {0.0};
+      const int op[1] = {kMax};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        v1[0] = smax(v1[0], fabs(cellDivergence(I, c, c % I.NI, c / I.NI)));
+      }
+      teamReduce(t, sh, v1, op);
+      mon[kMonMaxDivergence] = smax(0.0, v1[0]);
+    }
+
+    if (leader) {
+      for (int s = 0; s < kMonSlots; ++s) I.history[it * kMonSlots + s] = mon[s];
+    }
+    done = it + 1;
+    if (tolerance >= 0.0) {
+      const double a = mon[kMonContinuity], b = mon[kMonMomX], cc = mon[kMonMomY];
+      if (!isfinite(a) || !isfinite(b) || !isfinite(cc)) break;
+      if (smax(smax(fabs(a), fabs(b)), fabs(cc)) < tolerance) break;
+    }
+  }
+  if (leader) *I.iterations = done;
+  // No CTA may exit while a peer can still read its shared memory.
+  t.cl.sync();
+}
+
+/// Brute-force distance from each cell centroid to the nearest no-slip wall
+/// face centre (TurbulenceModel.cpp:28-65). One thread per cell.
+__global__ void wallDistanceKernel(int n, const double* __restrict__ centroid,
+                                   int walls, const double* __restrict__ wallCentre,
+                                   double far, double* __restrict__ out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  if (walls == 0) {
+    out[c] = far;
+    return;
+  }
+  const double cx = centroid[2 * c], cy = centroid[2 * c + 1];
+  double best = 1.7976931348623157e308;
+  for (int w = 0; w < walls; ++w) {
+    const double dx = cx - wallCentre[2 * w];
+    const double dy = cy - wallCentre[2 * w + 1];
+    const double sq = dx * dx + dy * dy;
+    best = smin(best, sq);
+  }
+  out[c] = sqrt(best);
+}
+
+}  // namespace cfdb
+
+// ---- launch helpers ---------------------------------------------------------------
+
+namespace cfdb {
+
+int chooseClusterSize(int cells) {
+  // About four cells per thread at 512 threads per CTA before another CTA is
+  // added; 16 is the largest (non-portable) cluster.
+  int r = 1;
+  while (r < 16 && cells > r * 512 * 4) r *= 2;
+  return r;
+}
+
+Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
+                    int iterations, int stopStage, double tolerance, cudaStream_t stream) {
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    configured = true;
+  }
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(static_cast<unsigned>(count * clusterSize), 1, 1);
+  config.blockDim = dim3(static_cast<unsigned>(threads), 1, 1);
+  config.dynamicSmemBytes = 0;
+  config.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = static_cast<unsigned>(clusterSize);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  config.attrs = attr;
+  config.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&config, simpleKernel, dInstances, iterations, stopStage, tolerance);
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, std::string("SIMPLE kernel launch: ") + cudaGetErrorString(e));
+  return CFD_OK;
+}
+
+Status launchWallDistance(int n, const double* centroid, int walls, const double* wallCentre,
+                          double far, double* out, cudaStream_t stream) {
+  const int block = 256;
+  wallDistanceKernel<<<(n + block - 1) / block, block, 0, stream>>>(n, centroid, walls, wallCentre, far, out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  return CFD_OK;
+}
+
+}  // namespace cfdb

@@ -1,0 +1,898 @@
+// solver.cu - host side of a device-resident SIMPLE solve and the C ABI
+// (include/cfd_gpu.h).
+
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <string>
+
+#include "cfd_gpu.h"
+
+namespace cfdb {
+
+Status launchWallDistance(int n, const double* centroid, int walls, const double* wallCentre,
+                          double far, double* out, cudaStream_t stream);
+
+namespace {
+thread_local std::string g_message;
+
+constexpr double kTinySolver = 1e-300;
+constexpr double kTinySst = 1.0e-30;
+constexpr double kMinOmega = 1.0e-10;
+
+inline double hyp(double x, double y) { return std::hypot(x, y); }
+
+#define CUDA_OR_FAIL(expr)                                                              \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e_)); \
+  } while (0)
+}  // namespace
+
+Status fail(Status code, const std::string& message) {
+  g_message = message;
+  return code;
+}
+
+// ---- settings -----------------------------------------------------------------
+
+Settings fromC(const cfd_settings& s) {
+  Settings o;
+  o.velocityRelaxation = s.velocity_relaxation;
+  o.pressureRelaxation = s.pressure_relaxation;
+  o.momentumSweeps = s.momentum_sweeps;
+  o.pressureIterations = s.pressure_iterations;
+  o.pressureTolerance = s.pressure_tolerance;
+  o.scheme = s.scheme;
+  o.turbulenceRelaxation = s.turbulence_relaxation;
+  o.inflowIntensity = s.inflow_intensity;
+  o.inflowViscosityRatio = s.inflow_viscosity_ratio;
+  o.inflowLengthScale = s.inflow_length_scale;
+  o.nonOrthogonalCorrectors = s.non_orthogonal_correctors;
+  o.nonOrthogonalBlend = s.non_orthogonal_blend;
+  o.precision = s.precision;
+  return o;
+}
+
+void toC(const Settings& s, cfd_settings* o) {
+  o->velocity_relaxation = s.velocityRelaxation;
+  o->pressure_relaxation = s.pressureRelaxation;
+  o->momentum_sweeps = s.momentumSweeps;
+  o->pressure_iterations = s.pressureIterations;
+  o->pressure_tolerance = s.pressureTolerance;
+  o->scheme = s.scheme;
+  o->turbulence_relaxation = s.turbulenceRelaxation;
+  o->inflow_intensity = s.inflowIntensity;
+  o->inflow_viscosity_ratio = s.inflowViscosityRatio;
+  o->inflow_length_scale = s.inflowLengthScale;
+  o->non_orthogonal_correctors = s.nonOrthogonalCorrectors;
+  o->non_orthogonal_blend = s.nonOrthogonalBlend;
+  o->precision = s.precision;
+}
+
+// ---- device arena ---------------------------------------------------------------
+
+DeviceArena::~DeviceArena() {
+  if (base_ != nullptr) cudaFree(base_);
+}
+
+Status DeviceArena::allocate() {
+  const std::size_t bytes = used_;
+  CUDA_OR_FAIL(cudaMalloc(reinterpret_cast<void**>(&base_), bytes));
+  CUDA_OR_FAIL(cudaMemset(base_, 0, bytes));
+  used_ = 0;
+  return CFD_OK;
+}
+
+// ---- create (SimpleSolver.cpp:30-131) -----------------------------------------------
+
+int Solver::idxOf(int f) const {
+  if (f < jFaces_) return f;
+  const int g = f - jFaces_;
+  const int i = g / NJ_, j = g % NJ_;
+  return j * (NI_ + 1) + i;
+}
+
+Status Solver::create(const cfd_mesh_desc& mesh, const cfd_face_bc& bc, const Settings& s,
+                      Solver** out) {
+  if (mesh.cell_count <= 0) return fail(CFD_INVALID_ARGUMENT, "cannot solve on an empty mesh");
+  if (bc.kind == nullptr || bc.velocity == nullptr || bc.pressure == nullptr) {
+    return fail(CFD_INVALID_ARGUMENT, "face conditions are missing");
+  }
+  if (!(s.velocityRelaxation > 0.0) || s.velocityRelaxation > 1.0 || !(s.pressureRelaxation > 0.0) ||
+      s.pressureRelaxation > 1.0) {
+    return fail(CFD_INVALID_ARGUMENT, "relaxation factors must lie in (0, 1]");
+  }
+  if (s.precision != 0) return fail(CFD_NOT_IMPLEMENTED, "only the plain FP64 form is available in this build");
+  auto* solver = new Solver;
+  solver->settings_ = s;
+  if (Status st = solver->build(mesh, bc); st != CFD_OK) {
+    delete solver;
+    return st;
+  }
+  *out = solver;
+  return CFD_OK;
+}
+
+Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
+  const int ni = m.nodes_i, nj = m.nodes_j;
+  if (ni < 2 || nj < 2) return fail(CFD_NOT_IMPLEMENTED, "the device solver needs a structured mesh (nodesI, nodesJ)");
+  NI_ = ni - 1;
+  NJ_ = nj - 1;
+  N_ = NI_ * NJ_;
+  jFaces_ = NI_ * nj;
+  F_ = jFaces_ + ni * NJ_;
+  if (m.cell_count != N_ || m.face_count != F_) {
+    return fail(CFD_INVALID_ARGUMENT, "cell or face count does not match the structured block");
+  }
+  const std::size_t N = N_, F = F_;
+  auto copyIn = [](const auto* src, std::size_t n, auto& dst) { dst.assign(src, src + n); };
+  copyIn(m.cell_centroids, 2 * N, centroid_);
+  copyIn(m.cell_areas, N, cellArea_);
+  copyIn(m.face_centres, 2 * F, faceCentre_);
+  copyIn(m.face_normals, 2 * F, faceNormal_);
+  copyIn(m.face_areas, F, faceArea_);
+  copyIn(m.face_owner, F, owner_);
+  copyIn(m.face_neighbour, F, neighbour_);
+  copyIn(m.face_boundary, F, boundary_);
+  copyIn(m.face_partner, F, partner_);
+  copyIn(bc.kind, F, kind_);
+  copyIn(bc.velocity, 2 * F, bcVel_);
+  copyIn(bc.pressure, F, bcP_);
+
+  // The structured layout of buildStructured (Mesh.cpp:138-170) is what the
+  // device indexing assumes; anything else is refused rather than misread.
+  for (int f = 0; f < F_; ++f) {
+    int o, n;
+    if (f < jFaces_) {
+      const int i = f % NI_, j = f / NI_;
+      o = (j == 0) ? i : (j == NJ_) ? (NJ_ - 1) * NI_ + i : (j - 1) * NI_ + i;
+      n = (j == 0 || j == NJ_) ? -1 : j * NI_ + i;
+    } else {
+      const int g = f - jFaces_, i = g / NJ_, j = g % NJ_;
+      o = (i == 0) ? j * NI_ : (i == NI_) ? j * NI_ + NI_ - 1 : j * NI_ + i - 1;
+      n = (i == 0 || i == NI_) ? -1 : j * NI_ + i;
+    }
+    if (owner_[f] != o || neighbour_[f] != n) {
+      return fail(CFD_NOT_IMPLEMENTED, "face " + std::to_string(f) + " is not in the structured block layout");
+    }
+    if (f >= NI_ && partner_[f] >= 0) {
+      return fail(CFD_NOT_IMPLEMENTED, "wake-cut partners are supported on the j = 0 boundary only");
+    }
+    if (kind_[f] < CFD_BC_INTERNAL || kind_[f] > CFD_BC_NOSLIP_WALL) {
+      return fail(CFD_INVALID_ARGUMENT, "unknown boundary kind on face " + std::to_string(f));
+    }
+  }
+
+  // oppositeCell (Mesh.cpp:78-87) and precomputeGeometry (SimpleSolver.cpp:82-131).
+  across_.assign(F, -1);
+  Sx_.assign(F, 0.0); Sy_.assign(F, 0.0); dx_.assign(F, 0.0); dy_.assign(F, 0.0);
+  D_.assign(F, 0.0); w_.assign(F, 1.0);
+  std::vector<double> Tx(F, 0.0), Ty(F, 0.0), Dt(F, 0.0);
+  for (std::size_t f = 0; f < F; ++f) {
+    if (neighbour_[f] >= 0) across_[f] = neighbour_[f];
+    else if (boundary_[f] == CFD_FACE_WAKECUT && partner_[f] >= 0) across_[f] = owner_[partner_[f]];
+    const double ax = faceNormal_[2 * f] * faceArea_[f];
+    const double ay = faceNormal_[2 * f + 1] * faceArea_[f];
+    Sx_[f] = ax;
+    Sy_[f] = ay;
+    const int o = owner_[f];
+    const double ocx = centroid_[2 * o], ocy = centroid_[2 * o + 1];
+    const double fcx = faceCentre_[2 * f], fcy = faceCentre_[2 * f + 1];
+    double ddx, ddy, w;
+    if (neighbour_[f] >= 0) {
+      const int n = neighbour_[f];
+      ddx = centroid_[2 * n] - ocx;
+      ddy = centroid_[2 * n + 1] - ocy;
+      // ownerWeight (Gradient.cpp:7-18)
+      const double toOwner = hyp(ocx - fcx, ocy - fcy);
+      const double toNb = hyp(centroid_[2 * n] - fcx, centroid_[2 * n + 1] - fcy);
+      const double total = toOwner + toNb;
+      w = (total > 0.0) ? toNb / total : 0.5;
+    } else if (across_[f] >= 0) {
+      const int a = across_[f];
+      ddx = centroid_[2 * a] - ocx;
+      ddy = centroid_[2 * a + 1] - ocy;
+      const double toOwner = hyp(ocx - fcx, ocy - fcy);
+      const double toAcross = hyp(centroid_[2 * a] - fcx, centroid_[2 * a + 1] - fcy);
+      const double span = toOwner + toAcross;
+      w = (span > 0.0) ? toAcross / span : 0.5;
+    } else {
+      ddx = fcx - ocx;
+      ddy = fcy - ocy;
+      w = 1.0;
+    }
+    dx_[f] = ddx;
+    dy_[f] = ddy;
+    w_[f] = w;
+    const double aDd = ax * ddx + ay * ddy;
+    const double aSq = ax * ax + ay * ay;
+    if (std::abs(aDd) > kTinySolver) {
+      D_[f] = aSq / aDd;
+      Tx[f] = ax - ddx * D_[f];
+      Ty[f] = ay - ddy * D_[f];
+    }
+    // KOmegaSST.cpp:399-403 / :423-427
+    Dt[f] = (std::abs(aDd) > kTinySst) ? std::abs(aSq / aDd) : 0.0;
+  }
+
+  // Red-black ordering needs the two cells across each wake pair to differ
+  // in colour (always true on a C-grid, where cellsI is even).
+  std::vector<int> acrossJ0(NI_, -1);
+  for (int i = 0; i < NI_; ++i) {
+    const int a = (neighbour_[i] < 0) ? across_[i] : -1;
+    acrossJ0[i] = a;
+    if (a >= 0) {
+      const int ai = a % NI_, aj = a / NI_;
+      if (((ai + aj) & 1) == (i & 1)) {
+        return fail(CFD_NOT_IMPLEMENTED, "wake-cut partners of equal colour (odd cellsI)");
+      }
+    }
+  }
+
+  bool anchor = false;
+  for (int f = 0; f < F_; ++f) {
+    if (kind_[f] == CFD_BC_OUTLET || kind_[f] == CFD_BC_FARFIELD) {
+      anchor = true;
+      break;
+    }
+  }
+  hasPRef_ = anchor;
+
+  // Wall faces: no-slip faces, marked on their owner (KOmegaSST.cpp:312-316).
+  std::vector<uint8_t> wallMask(N, 0);
+  std::vector<double> wallCentres;
+  for (int f = 0; f < F_; ++f) {
+    if (kind_[f] != CFD_BC_NOSLIP_WALL) continue;
+    wallCentres.push_back(faceCentre_[2 * f]);
+    wallCentres.push_back(faceCentre_[2 * f + 1]);
+    const int o = owner_[f];
+    const int oi = o % NI_, oj = o / NI_;
+    int bit;
+    if (f < jFaces_) bit = (f / NI_ == oj) ? 0 : 1;  // south (j = 0 row) or north
+    else bit = (((f - jFaces_) / NJ_) == oi) ? 2 : 3;  // west (i = 0) or east
+    wallMask[o] |= static_cast<uint8_t>(1u << bit);
+  }
+
+  // ---- device layout ----
+  const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
+  const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
+  historyCapacity_ = 256;
+  auto carve = [&](DeviceArena& a) {
+    Instance& I = view_;
+    I.vol = a.take<double>(N);
+    auto famGeo = [&](FaceGeo& g, std::size_t n) {
+      g.Sx = a.take<double>(n); g.Sy = a.take<double>(n); g.D = a.take<double>(n);
+      g.Tx = a.take<double>(n); g.Ty = a.take<double>(n); g.w = a.take<double>(n);
+      g.Dt = a.take<double>(n); g.nx = a.take<double>(n); g.ny = a.take<double>(n);
+    };
+    famGeo(I.gN, FN);
+    famGeo(I.gE, FE);
+    I.acrossJ0 = a.take<int>(NI_);
+    I.kindN = a.take<int8_t>(FN); I.kindE = a.take<int8_t>(FE);
+    I.bcuN = a.take<double>(FN); I.bcvN = a.take<double>(FN); I.bcpN = a.take<double>(FN);
+    I.bcuE = a.take<double>(FE); I.bcvE = a.take<double>(FE); I.bcpE = a.take<double>(FE);
+    I.deadN = a.take<double>(FN); I.deadE = a.take<double>(FE);
+    I.wallDist = a.take<double>(N);
+    I.wallMask = a.take<uint8_t>(N);
+    double** cellArrays[] = {&I.u, &I.v, &I.p, &I.rho, &I.mu, &I.muMol, &I.gux, &I.guy, &I.gvx,
+                             &I.gvy, &I.gpx, &I.gpy, &I.aD, &I.aS, &I.aN, &I.aW, &I.aE, &I.bU,
+                             &I.bV, &I.pD, &I.pB, &I.net, &I.x, &I.r, &I.z, &I.q, &I.d0, &I.d1,
+                             &I.div, &I.k, &I.om, &I.mut, &I.strain, &I.f1, &I.f2, &I.cd, &I.prod,
+                             &I.gkx, &I.gky, &I.gwx, &I.gwy, &I.kD, &I.kS, &I.kN, &I.kW, &I.kE,
+                             &I.kB, &I.wD, &I.wS, &I.wN, &I.wW, &I.wE, &I.wB};
+    for (double** ptr : cellArrays) *ptr = a.take<double>(N);
+    I.mfN = a.take<double>(FN); I.mfE = a.take<double>(FE);
+    I.pN = a.take<double>(FN); I.pE = a.take<double>(FE);
+    I.history = a.take<double>(static_cast<std::size_t>(historyCapacity_) * kMonSlots);
+    I.iterations = a.take<int>(1);
+    dCentroids_ = a.take<double>(2 * N);
+    dWallCentres_ = a.take<double>(std::max<std::size_t>(wallCentres.size(), 2));
+    dView_ = a.take<Instance>(1);
+  };
+  carve(arena_);
+  if (Status st = arena_.allocate(); st != CFD_OK) return st;
+  carve(arena_);
+  dHistory_ = view_.history;
+  dIterations_ = view_.iterations;
+  CUDA_OR_FAIL(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+
+  // Scatter per-face data into the two device families.
+  std::vector<double> hN(FN), hE(FE);
+  auto put = [&](const std::vector<double>& src, const double* dN, const double* dE) -> Status {
+    std::fill(hN.begin(), hN.end(), 0.0);
+    std::fill(hE.begin(), hE.end(), 0.0);
+    for (int f = 0; f < F_; ++f) (famOf(f) ? hE : hN)[idxOf(f)] = src[f];
+    CUDA_OR_FAIL(cudaMemcpy(const_cast<double*>(dN), hN.data(), FN * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_OR_FAIL(cudaMemcpy(const_cast<double*>(dE), hE.data(), FE * sizeof(double), cudaMemcpyHostToDevice));
+    return CFD_OK;
+  };
+  std::vector<double> nx(F), ny(F), bu(F), bv(F);
+  for (std::size_t f = 0; f < F; ++f) {
+    nx[f] = faceNormal_[2 * f];
+    ny[f] = faceNormal_[2 * f + 1];
+    bu[f] = bcVel_[2 * f];
+    bv[f] = bcVel_[2 * f + 1];
+  }
+  Instance& I = view_;
+  Status st = CFD_OK;
+  if ((st = put(Sx_, I.gN.Sx, I.gE.Sx)) || (st = put(Sy_, I.gN.Sy, I.gE.Sy)) ||
+      (st = put(D_, I.gN.D, I.gE.D)) || (st = put(Tx, I.gN.Tx, I.gE.Tx)) ||
+      (st = put(Ty, I.gN.Ty, I.gE.Ty)) || (st = put(w_, I.gN.w, I.gE.w)) ||
+      (st = put(Dt, I.gN.Dt, I.gE.Dt)) || (st = put(nx, I.gN.nx, I.gE.nx)) ||
+      (st = put(ny, I.gN.ny, I.gE.ny)) || (st = put(bu, I.bcuN, I.bcuE)) ||
+      (st = put(bv, I.bcvN, I.bcvE)) || (st = put(bcP_, I.bcpN, I.bcpE))) {
+    return st;
+  }
+  std::vector<int8_t> kN(FN, 0), kE(FE, 0);
+  for (int f = 0; f < F_; ++f) (famOf(f) ? kE : kN)[idxOf(f)] = static_cast<int8_t>(kind_[f]);
+  CUDA_OR_FAIL(cudaMemcpy(const_cast<int8_t*>(I.kindN), kN.data(), FN, cudaMemcpyHostToDevice));
+  CUDA_OR_FAIL(cudaMemcpy(const_cast<int8_t*>(I.kindE), kE.data(), FE, cudaMemcpyHostToDevice));
+  CUDA_OR_FAIL(cudaMemcpy(const_cast<int*>(I.acrossJ0), acrossJ0.data(), NI_ * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_OR_FAIL(cudaMemcpy(const_cast<double*>(I.vol), cellArea_.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  CUDA_OR_FAIL(cudaMemcpy(const_cast<uint8_t*>(I.wallMask), wallMask.data(), N, cudaMemcpyHostToDevice));
+  CUDA_OR_FAIL(cudaMemcpy(dCentroids_, centroid_.data(), 2 * N * sizeof(double), cudaMemcpyHostToDevice));
+  if (!wallCentres.empty()) {
+    CUDA_OR_FAIL(cudaMemcpy(dWallCentres_, wallCentres.data(), wallCentres.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  // momentumDiagonal_ starts at 1 (SimpleSolver.cpp:64).
+  {
+    std::vector<double> ones(N, 1.0);
+    CUDA_OR_FAIL(cudaMemcpy(I.aD, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  }
+
+  // Wall distance, once, on the device (TurbulenceModel.cpp:28-65).
+  double totalArea = 0.0;
+  for (double a : cellArea_) totalArea += a;
+  const double far = 1.0e6 * std::sqrt(std::abs(totalArea) + 1.0);
+  if ((st = launchWallDistance(N_, dCentroids_, static_cast<int>(wallCentres.size() / 2), dWallCentres_,
+                               far, const_cast<double*>(I.wallDist), stream_)) != CFD_OK) {
+    return st;
+  }
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+  wallDist_.resize(N);
+  CUDA_OR_FAIL(cudaMemcpy(wallDist_.data(), I.wallDist, N * sizeof(double), cudaMemcpyDeviceToHost));
+
+  clusterSize_ = chooseClusterSize(N_);
+  return uploadSettings();
+}
+
+Solver::~Solver() {
+  if (stream_ != nullptr) cudaStreamDestroy(stream_);
+}
+
+Status Solver::uploadSettings() {
+  Instance& I = view_;
+  I.NI = NI_;
+  I.NJ = NJ_;
+  I.N = N_;
+  I.model = model_;
+  I.alphaU = settings_.velocityRelaxation;
+  I.alphaP = settings_.pressureRelaxation;
+  I.blend = settings_.nonOrthogonalBlend;
+  I.alphaT = settings_.turbulenceRelaxation;
+  I.sweeps = settings_.momentumSweeps;
+  I.cgMax = settings_.pressureIterations;
+  I.cgTol = settings_.pressureTolerance;
+  I.sou = (settings_.scheme != 0) ? 1 : 0;
+  I.nCorr = settings_.nonOrthogonalCorrectors;
+  I.hasPRef = hasPRef_ ? 1 : 0;
+  I.refMassFlow = refMassFlow_;
+  I.kIn = kIn_;
+  I.wIn = wIn_;
+  // SSTConstants::gamma1/gamma2 (KOmegaSST.cpp:96-102) and beta*^(1/4).
+  const double beta1 = 0.075, beta2 = 0.0828, betaStar = 0.09, kappa = 0.41;
+  I.gamma1 = beta1 / betaStar - 0.5 * kappa * kappa / std::sqrt(betaStar);
+  I.gamma2 = beta2 / betaStar - 0.856 * kappa * kappa / std::sqrt(betaStar);
+  I.betaStarQuarter = std::pow(betaStar, 0.25);
+  CUDA_OR_FAIL(cudaMemcpy(dView_, &view_, sizeof(Instance), cudaMemcpyHostToDevice));
+  return CFD_OK;
+}
+
+Status Solver::setSettings(const Settings& s) {
+  if (!(s.velocityRelaxation > 0.0) || s.velocityRelaxation > 1.0 || !(s.pressureRelaxation > 0.0) ||
+      s.pressureRelaxation > 1.0) {
+    return fail(CFD_INVALID_ARGUMENT, "relaxation factors must lie in (0, 1]");
+  }
+  if (s.precision != 0) return fail(CFD_NOT_IMPLEMENTED, "only the plain FP64 form is available in this build");
+  settings_ = s;
+  return uploadSettings();
+}
+
+Status Solver::download(const double* dev, std::size_t n, double* host) {
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+  CUDA_OR_FAIL(cudaMemcpy(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return CFD_OK;
+}
+
+Status Solver::upload(double* dev, const double* host, std::size_t n) {
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+  CUDA_OR_FAIL(cudaMemcpy(dev, host, n * sizeof(double), cudaMemcpyHostToDevice));
+  return CFD_OK;
+}
+
+// ---- initialise (SimpleSolver.cpp:133-210) ------------------------------------------
+
+Status Solver::initialise(const double* u, const double* v, const double* p, const double* rho,
+                          const double* mu) {
+  if (u == nullptr || v == nullptr || p == nullptr || rho == nullptr || mu == nullptr) {
+    return fail(CFD_INVALID_ARGUMENT, "initial field has missing arrays");
+  }
+  const std::size_t N = N_, F = F_;
+  muMol_.assign(mu, mu + N);
+  // Current fluxes decide imposesVelocity during the seed, as in the reference.
+  std::vector<double> flux(F, 0.0);
+  if (Status st = readField(CFD_FIELD_MASS_FLUX, flux.data()); st != CFD_OK) return st;
+
+  double speed = 0.0;
+  for (std::size_t c = 0; c < N; ++c) speed = std::max(speed, hyp(u[c], v[c]));
+  std::vector<double> dead(F, 0.0);
+  for (std::size_t f = 0; f < F; ++f) {
+    if (kind_[f] != CFD_BC_FARFIELD) continue;
+    dead[f] = 1.0e-3 * rho[owner_[f]] * speed * hyp(Sx_[f], Sy_[f]);
+  }
+  auto imposes = [&](std::size_t f) {
+    switch (kind_[f]) {
+      case CFD_BC_NOSLIP_WALL:
+      case CFD_BC_INLET: return true;
+      case CFD_BC_FARFIELD: return flux[f] < dead[f];
+      default: return false;
+    }
+  };
+  std::vector<double> seeded(F, 0.0);
+  for (std::size_t f = 0; f < F; ++f) {
+    const int o = owner_[f];
+    const int other = across_[f];
+    double fu, fv;
+    if (other >= 0) {
+      const double w = w_[f];
+      fu = w * u[o] + (1.0 - w) * u[other];
+      fv = w * v[o] + (1.0 - w) * v[other];
+    } else if (imposes(f)) {
+      fu = bcVel_[2 * f];
+      fv = bcVel_[2 * f + 1];
+    } else {
+      fu = u[o];
+      fv = v[o];
+    }
+    double density = rho[o];
+    if (neighbour_[f] >= 0) {
+      const double w = w_[f];
+      density = w * rho[o] + (1.0 - w) * rho[neighbour_[f]];
+    }
+    seeded[f] = density * (fu * Sx_[f] + fv * Sy_[f]);
+  }
+  double ref = 0.0;
+  for (std::size_t f = 0; f < F; ++f) {
+    if (boundary_[f] == CFD_FACE_INTERIOR || kind_[f] == CFD_BC_INTERNAL) continue;
+    ref += std::max(-seeded[f], 0.0);
+  }
+  if (!(ref > 0.0)) ref = 1.0;
+  refMassFlow_ = ref;
+
+  Instance& I = view_;
+  Status st = CFD_OK;
+  if ((st = upload(I.u, u, N)) || (st = upload(I.v, v, N)) || (st = upload(I.p, p, N)) ||
+      (st = upload(I.rho, rho, N)) || (st = upload(I.mu, mu, N)) || (st = upload(I.muMol, mu, N))) {
+    return st;
+  }
+  {
+    const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
+    const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
+    std::vector<double> hN(FN, 0.0), hE(FE, 0.0), dN(FN, 0.0), dE(FE, 0.0);
+    for (int f = 0; f < F_; ++f) {
+      (famOf(f) ? hE : hN)[idxOf(f)] = seeded[f];
+      (famOf(f) ? dE : dN)[idxOf(f)] = dead[f];
+    }
+    if ((st = upload(I.mfN, hN.data(), FN)) || (st = upload(I.mfE, hE.data(), FE)) ||
+        (st = upload(const_cast<double*>(I.deadN), dN.data(), FN)) ||
+        (st = upload(const_cast<double*>(I.deadE), dE.data(), FE))) {
+      return st;
+    }
+  }
+  initialised_ = true;
+  if (model_ == 2) {
+    if ((st = sstInitialise()) != CFD_OK) return st;
+  } else if (model_ == 1) {
+    // LaminarModel: mu_t = 0, so mu_eff = mu + 0 (TurbulenceModel.cpp:67-71).
+    std::vector<double> eff(N);
+    for (std::size_t c = 0; c < N; ++c) eff[c] = muMol_[c] + 0.0;
+    if ((st = upload(I.mu, eff.data(), N)) != CFD_OK) return st;
+  }
+  return uploadSettings();
+}
+
+// ---- KOmegaSST::initialise (KOmegaSST.cpp:104-200) ------------------------------------
+
+Status Solver::sstInitialise() {
+  const std::size_t N = N_;
+  const Settings& s = settings_;
+  if (!std::isfinite(s.inflowIntensity) || s.inflowIntensity < 0.0) {
+    return fail(CFD_INVALID_ARGUMENT, "turbulence intensity must be finite and not negative");
+  }
+  if (!std::isfinite(s.inflowViscosityRatio) || s.inflowViscosityRatio <= 0.0) {
+    return fail(CFD_INVALID_ARGUMENT, "the eddy viscosity ratio must be positive");
+  }
+  if (!std::isfinite(s.inflowLengthScale) || s.inflowLengthScale < 0.0) {
+    return fail(CFD_INVALID_ARGUMENT, "the turbulence length scale must not be negative");
+  }
+  // The model initialises from the field as the solver holds it now: the
+  // effective viscosity is what the reference passes (field_.viscosity).
+  std::vector<double> u(N), v(N), rho(N), mu(N);
+  Instance& I = view_;
+  Status st = CFD_OK;
+  if ((st = download(I.u, N, u.data())) || (st = download(I.v, N, v.data())) ||
+      (st = download(I.rho, N, rho.data())) || (st = download(I.mu, N, mu.data()))) {
+    return st;
+  }
+  double refSpeed = 0.0, refRho = 0.0, refMu = 0.0;
+  for (std::size_t c = 0; c < N; ++c) {
+    const double sp = hyp(u[c], v[c]);
+    if (sp > refSpeed) refSpeed = sp;
+    refRho = std::max(refRho, rho[c]);
+    refMu = std::max(refMu, mu[c]);
+  }
+  if (!(refSpeed > 0.0) || !(refRho > 0.0) || !(refMu > 0.0)) {
+    return fail(CFD_INVALID_ARGUMENT, "the starting field has no scale to set freestream turbulence from");
+  }
+  const double betaStar = 0.09, beta1 = 0.075, kappa = 0.41;
+  const double intensity = std::max(s.inflowIntensity, 1.0e-8);
+  kIn_ = 1.5 * (intensity * refSpeed) * (intensity * refSpeed);
+  double eddy = 0.0;
+  if (s.inflowLengthScale > 0.0) {
+    wIn_ = std::max(std::sqrt(kIn_) / (std::pow(betaStar, 0.25) * s.inflowLengthScale), kMinOmega);
+    eddy = refRho * kIn_ / wIn_;
+  } else {
+    eddy = s.inflowViscosityRatio * refMu;
+    wIn_ = std::max(refRho * kIn_ / eddy, kMinOmega);
+  }
+  (void)eddy;
+  std::vector<double> k(N, kIn_), om(N, wIn_), mut(N), eff(N);
+  for (std::size_t c = 0; c < N; ++c) {
+    const double d = std::max(wallDist_[c], kTinySst);
+    const double nu = mu[c] / std::max(rho[c], kTinySst);
+    // wallOmega (KOmegaSST.cpp:86-92)
+    const double dd = std::max(d, kTinySst);
+    const double viscous = 6.0 * nu / (beta1 * dd * dd);
+    const double logarithmic = std::sqrt(std::max(k[c], 0.0)) / (std::pow(betaStar, 0.25) * kappa * dd);
+    const double wall = std::sqrt(viscous * viscous + logarithmic * logarithmic);
+    om[c] = std::max(wIn_, wall);
+    mut[c] = rho[c] * k[c] / om[c];
+    eff[c] = muMol_[c] + mut[c];
+  }
+  if ((st = upload(I.k, k.data(), N)) || (st = upload(I.om, om.data(), N)) ||
+      (st = upload(I.mut, mut.data(), N)) || (st = upload(I.mu, eff.data(), N))) {
+    return st;
+  }
+  return uploadSettings();
+}
+
+// ---- setTurbulenceModel (SimpleSolver.cpp:212-230) -------------------------------------
+
+Status Solver::setTurbulence(int model) {
+  if (model < 0 || model > 2) return fail(CFD_INVALID_ARGUMENT, "unknown turbulence model");
+  const int previous = model_;
+  model_ = model;
+  if (model == 0) {
+    if (initialised_) {
+      if (Status st = upload(view_.mu, muMol_.data(), N_); st != CFD_OK) return st;
+    }
+    return uploadSettings();
+  }
+  if (!initialised_) return uploadSettings();
+  (void)previous;
+  if (model == 1) {
+    std::vector<double> eff(N_);
+    for (int c = 0; c < N_; ++c) eff[c] = muMol_[c] + 0.0;
+    if (Status st = upload(view_.mu, eff.data(), N_); st != CFD_OK) return st;
+    return uploadSettings();
+  }
+  return sstInitialise();
+}
+
+// ---- iterate ---------------------------------------------------------------------------
+
+Status Solver::iterate(int n, int stopStage, double tolerance, std::vector<double>* history, int* taken) {
+  if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
+  if (n < 0) return fail(CFD_INVALID_ARGUMENT, "negative iteration count");
+  if (history != nullptr) history->clear();
+  int total = 0;
+  while (total < n) {
+    const int chunk = std::min(n - total, historyCapacity_);
+    if (Status st = launchSimple(dView_, 1, clusterSize_, threads_, chunk, stopStage, tolerance, stream_);
+        st != CFD_OK) {
+      return st;
+    }
+    CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+    int ran = 0;
+    CUDA_OR_FAIL(cudaMemcpy(&ran, dIterations_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (history != nullptr && ran > 0) {
+      const std::size_t old = history->size();
+      history->resize(old + static_cast<std::size_t>(ran) * kMonSlots);
+      CUDA_OR_FAIL(cudaMemcpy(history->data() + old, dHistory_, static_cast<std::size_t>(ran) * kMonSlots * sizeof(double),
+                              cudaMemcpyDeviceToHost));
+    }
+    total += ran;
+    if (ran < chunk || stopStage != kStageEnd) break;
+  }
+  if (taken != nullptr) *taken = total;
+  return CFD_OK;
+}
+
+// ---- field access -------------------------------------------------------------------
+
+Status Solver::readField(int which, double* out) {
+  if (out == nullptr) return fail(CFD_INVALID_ARGUMENT, "null output");
+  const Instance& I = view_;
+  const std::size_t N = N_, F = F_;
+  const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
+  const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
+  auto cell = [&](const double* dev) { return download(dev, N, out); };
+  auto faces = [&](const double* dN, const double* dE) -> Status {
+    std::vector<double> hN(FN), hE(FE);
+    if (Status st = download(dN, FN, hN.data()); st != CFD_OK) return st;
+    if (Status st = download(dE, FE, hE.data()); st != CFD_OK) return st;
+    for (int f = 0; f < F_; ++f) out[f] = (famOf(f) ? hE : hN)[idxOf(f)];
+    return CFD_OK;
+  };
+  auto vec2 = [&](const double* dx, const double* dy) -> Status {
+    std::vector<double> hx(N), hy(N);
+    if (Status st = download(dx, N, hx.data()); st != CFD_OK) return st;
+    if (Status st = download(dy, N, hy.data()); st != CFD_OK) return st;
+    for (std::size_t c = 0; c < N; ++c) {
+      out[2 * c] = hx[c];
+      out[2 * c + 1] = hy[c];
+    }
+    return CFD_OK;
+  };
+  auto rowsToFaces = [&](bool upper) -> Status {
+    // Row storage (S, N, W, E coefficients of each cell) back to the LDU
+    // upper/lower per face of LinearSystem.hpp:29-71.
+    std::vector<double> aS(N), aN(N), aW(N), aE(N);
+    Status st = CFD_OK;
+    if ((st = download(I.aS, N, aS.data())) || (st = download(I.aN, N, aN.data())) ||
+        (st = download(I.aW, N, aW.data())) || (st = download(I.aE, N, aE.data()))) {
+      return st;
+    }
+    for (std::size_t f = 0; f < F; ++f) {
+      out[f] = 0.0;
+      const int o = owner_[f], n = neighbour_[f];
+      if (n >= 0) {
+        if (static_cast<int>(f) < jFaces_) out[f] = upper ? aN[o] : aS[n];
+        else out[f] = upper ? aE[o] : aW[n];
+      } else if (across_[f] >= 0 && upper) {
+        out[f] = aS[o];
+      }
+    }
+    return CFD_OK;
+  };
+  switch (which) {
+    case CFD_FIELD_U: return cell(I.u);
+    case CFD_FIELD_V: return cell(I.v);
+    case CFD_FIELD_P: return cell(I.p);
+    case CFD_FIELD_RHO: return cell(I.rho);
+    case CFD_FIELD_MU_EFF: return cell(I.mu);
+    case CFD_FIELD_MASS_FLUX: return faces(I.mfN, I.mfE);
+    case CFD_FIELD_DIVERGENCE: {
+      // SimpleSolver::divergence (SimpleSolver.cpp:796-817), on the host.
+      std::vector<double> flux(F), rho(N);
+      Status st = CFD_OK;
+      if ((st = faces(I.mfN, I.mfE)) != CFD_OK) return st;
+      std::copy(out, out + F, flux.begin());
+      if ((st = download(I.rho, N, rho.data())) != CFD_OK) return st;
+      std::fill(out, out + N, 0.0);
+      for (std::size_t f = 0; f < F; ++f) {
+        const int o = owner_[f];
+        const double vf = flux[f] / std::max(rho[o], kTinySolver);
+        out[o] += vf;
+        if (neighbour_[f] >= 0) out[neighbour_[f]] -= vf;
+      }
+      for (std::size_t c = 0; c < N; ++c) out[c] = (cellArea_[c] > 0.0) ? out[c] / cellArea_[c] : 0.0;
+      return CFD_OK;
+    }
+    case CFD_FIELD_MU_MOLECULAR: return cell(I.muMol);
+    case CFD_FIELD_GRAD_U: return vec2(I.gux, I.guy);
+    case CFD_FIELD_GRAD_V: return vec2(I.gvx, I.gvy);
+    case CFD_FIELD_GRAD_P: return vec2(I.gpx, I.gpy);
+    case CFD_FIELD_MOM_DIAG: return cell(I.aD);
+    case CFD_FIELD_MOM_SOURCE_U: return cell(I.bU);
+    case CFD_FIELD_MOM_SOURCE_V: return cell(I.bV);
+    case CFD_FIELD_MOM_UPPER: return rowsToFaces(true);
+    case CFD_FIELD_MOM_LOWER: return rowsToFaces(false);
+    case CFD_FIELD_MOMENTUM_DIAGONAL: return cell(I.aD);
+    case CFD_FIELD_P_DIAG: return cell(I.pD);
+    case CFD_FIELD_P_SOURCE: return cell(I.pB);
+    case CFD_FIELD_P_UPPER: return faces(I.pN, I.pE);
+    case CFD_FIELD_NET_FLUX: return cell(I.net);
+    case CFD_FIELD_P_CORRECTION: return cell(I.x);
+    case CFD_FIELD_K: return cell(I.k);
+    case CFD_FIELD_OMEGA: return cell(I.om);
+    case CFD_FIELD_MUT: return cell(I.mut);
+    case CFD_FIELD_WALL_DISTANCE: return cell(I.wallDist);
+    case CFD_FIELD_STRAIN: return cell(I.strain);
+    case CFD_FIELD_F1: return cell(I.f1);
+    case CFD_FIELD_F2: return cell(I.f2);
+    case CFD_FIELD_CROSS_DIFFUSION: return cell(I.cd);
+    case CFD_FIELD_PRODUCTION: return cell(I.prod);
+    case CFD_FIELD_GRAD_K: return vec2(I.gkx, I.gky);
+    case CFD_FIELD_GRAD_OMEGA: return vec2(I.gwx, I.gwy);
+    case CFD_FIELD_T_DIAG_K: return cell(I.kD);
+    case CFD_FIELD_T_SOURCE_K: return cell(I.kB);
+    case CFD_FIELD_T_DIAG_W: return cell(I.wD);
+    case CFD_FIELD_T_SOURCE_W: return cell(I.wB);
+    default: break;
+  }
+  return fail(CFD_OUT_OF_RANGE, "unknown field " + std::to_string(which));
+}
+
+Status Solver::loadState(const double* u, const double* v, const double* p, const double* massFlux,
+                         const double* k, const double* omega, const double* mut, const double* muEff) {
+  if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
+  const Instance& I = view_;
+  const std::size_t N = N_;
+  Status st = CFD_OK;
+  if (u != nullptr && (st = upload(I.u, u, N))) return st;
+  if (v != nullptr && (st = upload(I.v, v, N))) return st;
+  if (p != nullptr && (st = upload(I.p, p, N))) return st;
+  if (massFlux != nullptr) {
+    const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
+    const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
+    std::vector<double> hN(FN, 0.0), hE(FE, 0.0);
+    for (int f = 0; f < F_; ++f) (famOf(f) ? hE : hN)[idxOf(f)] = massFlux[f];
+    if ((st = upload(I.mfN, hN.data(), FN)) || (st = upload(I.mfE, hE.data(), FE))) return st;
+  }
+  if (k != nullptr && (st = upload(I.k, k, N))) return st;
+  if (omega != nullptr && (st = upload(I.om, omega, N))) return st;
+  if (mut != nullptr && (st = upload(I.mut, mut, N))) return st;
+  if (muEff != nullptr && (st = upload(I.mu, muEff, N))) return st;
+  return CFD_OK;
+}
+
+}  // namespace cfdb
+
+// ---- C ABI ----------------------------------------------------------------------------
+
+struct cfd_solver_t {
+  cfdb::Solver* solver{nullptr};
+};
+
+namespace {
+void packMonitor(const double* h, cfd_monitor* m) {
+  using namespace cfdb;
+  m->continuity = h[kMonContinuity];
+  m->momentum_x = h[kMonMomX];
+  m->momentum_y = h[kMonMomY];
+  m->mass_imbalance = h[kMonMassImbalance];
+  m->max_divergence = h[kMonMaxDivergence];
+  m->pressure_iterations = static_cast<int>(h[kMonPressureIterations]);
+  m->pad_ = 0;
+  m->turbulence_first = h[kMonTurbFirst];
+  m->turbulence_second = h[kMonTurbSecond];
+  m->min_energy = h[kMonMinK];
+  m->max_energy = h[kMonMaxK];
+  m->min_dissipation = h[kMonMinW];
+  m->max_dissipation = h[kMonMaxW];
+  m->min_eddy_viscosity = h[kMonMinMut];
+  m->max_eddy_viscosity = h[kMonMaxMut];
+  m->max_eddy_viscosity_ratio = h[kMonMaxRatio];
+  m->max_wall_yplus = h[kMonMaxYPlus];
+}
+
+cfd_status checkHandle(cfd_handle h) {
+  if (h == nullptr || h->solver == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null solver handle");
+  return CFD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+const char* cfd_last_error(void) { return cfdb::g_message.c_str(); }
+
+void cfd_default_settings(cfd_settings* out) {
+  if (out != nullptr) cfdb::toC(cfdb::Settings{}, out);
+}
+
+cfd_status cfd_gpu_create(const cfd_mesh_desc* mesh, const cfd_face_bc* conditions,
+                          const cfd_settings* settings, cfd_handle* out) {
+  if (mesh == nullptr || conditions == nullptr || out == nullptr) {
+    return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  }
+  const cfdb::Settings s = (settings != nullptr) ? cfdb::fromC(*settings) : cfdb::Settings{};
+  cfdb::Solver* solver = nullptr;
+  if (cfd_status st = cfdb::Solver::create(*mesh, *conditions, s, &solver); st != CFD_OK) return st;
+  *out = new cfd_solver_t{solver};
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_set_turbulence(cfd_handle h, int model) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  return h->solver->setTurbulence(model);
+}
+
+cfd_status cfd_gpu_initialise(cfd_handle h, const double* u, const double* v, const double* p,
+                              const double* rho, const double* mu) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  return h->solver->initialise(u, v, p, rho, mu);
+}
+
+cfd_status cfd_gpu_iterate(cfd_handle h, int n, cfd_monitor* last, cfd_monitor* history) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  std::vector<double> hist;
+  int taken = 0;
+  if (cfd_status st = h->solver->iterate(n, cfdb::kStageEnd, -1.0, &hist, &taken); st != CFD_OK) return st;
+  if (history != nullptr) {
+    for (int k = 0; k < taken; ++k) packMonitor(hist.data() + k * cfdb::kMonSlots, history + k);
+  }
+  if (last != nullptr && taken > 0) packMonitor(hist.data() + (taken - 1) * cfdb::kMonSlots, last);
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_converge(cfd_handle h, int cap, double tol, int* taken, cfd_monitor* last) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  if (!(tol >= 0.0)) return cfdb::fail(CFD_INVALID_ARGUMENT, "tolerance must be >= 0");
+  std::vector<double> hist;
+  int ran = 0;
+  if (cfd_status st = h->solver->iterate(cap, cfdb::kStageEnd, tol, &hist, &ran); st != CFD_OK) return st;
+  if (taken != nullptr) *taken = ran;
+  if (last != nullptr && ran > 0) packMonitor(hist.data() + (ran - 1) * cfdb::kMonSlots, last);
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_iterate_partial(cfd_handle h, int stage, cfd_monitor* last) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  if (stage < 0 || stage > CFD_STAGE_END) return cfdb::fail(CFD_OUT_OF_RANGE, "unknown stage");
+  std::vector<double> hist;
+  int taken = 0;
+  if (cfd_status st = h->solver->iterate(1, stage, -1.0, &hist, &taken); st != CFD_OK) return st;
+  if (last != nullptr && taken > 0 && hist.size() >= static_cast<std::size_t>(cfdb::kMonSlots)) {
+    packMonitor(hist.data(), last);
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_read_field(cfd_handle h, int which, double* out) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  return h->solver->readField(which, out);
+}
+
+cfd_status cfd_gpu_load_state(cfd_handle h, const double* u, const double* v, const double* p,
+                              const double* mass_flux, const double* k, const double* omega,
+                              const double* mut, const double* mu_eff) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  return h->solver->loadState(u, v, p, mass_flux, k, omega, mut, mu_eff);
+}
+
+cfd_status cfd_gpu_set_settings(cfd_handle h, const cfd_settings* settings) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  if (settings == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null settings");
+  return h->solver->setSettings(cfdb::fromC(*settings));
+}
+
+cfd_status cfd_gpu_dims(cfd_handle h, int* out4) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  out4[0] = h->solver->cellsI();
+  out4[1] = h->solver->cellsJ();
+  out4[2] = h->solver->cells();
+  out4[3] = h->solver->faces();
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_scalars(cfd_handle h, double* out3) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  out3[0] = h->solver->kInflow();
+  out3[1] = h->solver->omegaInflow();
+  out3[2] = h->solver->referenceMassFlow();
+  return CFD_OK;
+}
+
+cfd_status cfd_gpu_destroy(cfd_handle h) {
+  if (h == nullptr) return CFD_OK;
+  delete h->solver;
+  delete h;
+  return CFD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// solver.hpp - host front end of one device-resident SIMPLE solve.
+//
+// Mirrors cfd::solver::SimpleSolver (include/cfd/solver/SimpleSolver.hpp:159-274):
+// create / setTurbulenceModel / initialise / iterate / field / massFlux /
+// divergence / setSettings, with the same validation and error codes. The
+// one-time set-up steps (precomputeGeometry, initialise's dead band, flux
+// seed and reference mass flow, KOmegaSST::initialise) run here on the host in
+// the reference's order, so the state the device starts from is the
+// reference's to the last bit. Everything per iteration runs on the device.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.hpp"
+#include "instance.hpp"
+
+namespace cfdb {
+
+/// One cudaMalloc carved into aligned arrays; released as a whole.
+class DeviceArena {
+ public:
+  DeviceArena() = default;
+  DeviceArena(const DeviceArena&) = delete;
+  DeviceArena& operator=(const DeviceArena&) = delete;
+  ~DeviceArena();
+  /// Reserve space for an array during sizing (pass 1) or hand it out (pass 2).
+  template <typename T>
+  T* take(std::size_t count) {
+    const std::size_t bytes = (count * sizeof(T) + 255) & ~std::size_t{255};
+    T* out = (base_ == nullptr) ? nullptr : reinterpret_cast<T*>(base_ + used_);
+    used_ += bytes;
+    return out;
+  }
+  Status allocate();  // after a sizing pass: one allocation, zero-filled
+  void rewind() { used_ = 0; }
+  std::size_t bytes() const { return used_; }
+
+ private:
+  char* base_{nullptr};
+  std::size_t used_{0};
+};
+
+struct Settings {
+  double velocityRelaxation{0.5};
+  double pressureRelaxation{0.2};
+  int momentumSweeps{3};
+  int pressureIterations{200};
+  double pressureTolerance{0.01};
+  int scheme{0};
+  double turbulenceRelaxation{0.5};
+  double inflowIntensity{0.001};
+  double inflowViscosityRatio{1.0};
+  double inflowLengthScale{0.0};
+  int nonOrthogonalCorrectors{1};
+  double nonOrthogonalBlend{1.0};
+  int precision{0};
+};
+
+Settings fromC(const cfd_settings& s);
+void toC(const Settings& s, cfd_settings* out);
+
+class Solver {
+ public:
+  static Status create(const cfd_mesh_desc& mesh, const cfd_face_bc& bc, const Settings& s,
+                       Solver** out);
+  ~Solver();
+
+  Status setTurbulence(int model);
+  Status initialise(const double* u, const double* v, const double* p, const double* rho,
+                    const double* mu);
+  /// n iterations (stopStage = kStageEnd), or one partial one; tolerance < 0
+  /// disables the convergence stop. history gets kMonSlots doubles per
+  /// iteration run; *taken the number run.
+  Status iterate(int n, int stopStage, double tolerance, std::vector<double>* history, int* taken);
+  Status readField(int which, double* out);
+  Status loadState(const double* u, const double* v, const double* p, const double* massFlux,
+                   const double* k, const double* omega, const double* mut, const double* muEff);
+  Status setSettings(const Settings& s);
+
+  int cellsI() const { return NI_; }
+  int cellsJ() const { return NJ_; }
+  int cells() const { return N_; }
+  int faces() const { return F_; }
+  double kInflow() const { return kIn_; }
+  double omegaInflow() const { return wIn_; }
+  double referenceMassFlow() const { return refMassFlow_; }
+  int clusterSize() const { return clusterSize_; }
+  const Instance& deviceView() const { return view_; }
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  Solver() = default;
+  Status build(const cfd_mesh_desc& mesh, const cfd_face_bc& bc);
+  Status sstInitialise();
+  Status uploadSettings();
+  Status download(const double* dev, std::size_t n, double* host);
+  Status upload(double* dev, const double* host, std::size_t n);
+  /// Reference face f -> (family, index) of the device layout.
+  int famOf(int f) const { return (f < jFaces_) ? 0 : 1; }
+  int idxOf(int f) const;
+
+  int NI_{0}, NJ_{0}, N_{0}, F_{0}, jFaces_{0};
+  Settings settings_{};
+  int model_{0};
+  bool initialised_{false};
+  bool hasPRef_{false};
+  double refMassFlow_{1.0};
+  double kIn_{0.0}, wIn_{0.0};
+
+  // host copies of the metrics the one-time steps need (reference order)
+  std::vector<double> centroid_, cellArea_, faceCentre_, faceNormal_, faceArea_;
+  std::vector<int> owner_, neighbour_, boundary_, partner_;
+  std::vector<int> kind_;
+  std::vector<double> bcVel_, bcP_;
+  std::vector<double> Sx_, Sy_, dx_, dy_, D_, w_;  // per reference face
+  std::vector<int> across_;                          // oppositeCell per face
+  std::vector<double> muMol_;
+  std::vector<double> wallDist_;
+
+  DeviceArena arena_;
+  Instance view_{};
+  Instance* dView_{nullptr};
+  double* dHistory_{nullptr};
+  int* dIterations_{nullptr};
+  int historyCapacity_{0};
+  double* dWallCentres_{nullptr};
+  double* dCentroids_{nullptr};
+  cudaStream_t stream_{nullptr};
+  int clusterSize_{8};
+  int threads_{512};
+};
+
+/// Launch the SIMPLE kernel over `count` instances (device array), one
+/// cluster of `clusterSize` CTAs each.
+Status launchWallDistance(int n, const double* centroid, int walls, const double* wallCentre,
+                          double far, double* out, cudaStream_t stream);
+
+Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
+                    int iterations, int stopStage, double tolerance, cudaStream_t stream);
+
+/// Cluster size used for a solve of `cells` cells (power of two, 1..16).
+int chooseClusterSize(int cells);
+
+}  // namespace cfdb

@@ -1,0 +1,194 @@
+/* cfd_gpu.h - C ABI of the B200 steady SIMPLE solver (laminar and k-omega SST)
+ * on structured C-grids.
+ *
+ * This is the boundary a host program binds to. It replaces the internals of
+ * the reference's C++ class cfd::solver::SimpleSolver and its TurbulenceModel
+ * plug-in (include/cfd/solver/SimpleSolver.hpp:159-274,
+ * include/cfd/solver/TurbulenceModel.hpp:155-206, include/cfd/solver/KOmegaSST.hpp:174-257).
+ * Plain pointers and sizes only. Every array is FP64 and in the reference's
+ * own ordering: cells c = j*cellsI + i (Mesh::cellIndex, Mesh.hpp:168), faces
+ * j-faces first then i-faces (Mesh.cpp:138-156), Vec2 arrays as (x, y) pairs.
+ *
+ * Errors: every entry point returns a cfd_status. Non-zero codes map one to
+ * one onto cfd::ErrorCode (include/cfd/core/Error.hpp:37-46) plus one; the
+ * message of the last failure on the calling thread is cfd_last_error().
+ * As in the reference, a diverging solve is not an error: it shows up as
+ * non-finite residuals in the monitor (src/app/SolverWorker.cpp:169-181).
+ *
+ * Threading: a handle is single-owner, like SimpleSolver. Calls on one handle
+ * come from one host thread at a time. A handle owns one CUDA stream.
+ */
+#ifndef CFD_GPU_H
+#define CFD_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int cfd_status;
+enum {
+  CFD_OK = 0,
+  CFD_INVALID_ARGUMENT = 1, /* ErrorCode::InvalidArgument */
+  CFD_OUT_OF_RANGE = 2,
+  CFD_NOT_FOUND = 3,
+  CFD_IO_FAILURE = 4,
+  CFD_NOT_IMPLEMENTED = 5,
+  CFD_INITIALIZATION_FAILURE = 6, /* also: CUDA device or allocation failure */
+  CFD_NUMERICAL_FAILURE = 7,
+  CFD_INTERNAL = 8
+};
+
+typedef struct cfd_solver_t* cfd_handle;
+
+/* flow::BoundaryKind (include/cfd/flow/BoundaryConditions.hpp:34-72). */
+enum { CFD_BC_INTERNAL = 0, CFD_BC_INLET = 1, CFD_BC_OUTLET = 2, CFD_BC_FARFIELD = 3,
+       CFD_BC_NOSLIP_WALL = 4 };
+/* mesh::BoundaryType (include/cfd/mesh/Mesh.hpp:42-48). */
+enum { CFD_FACE_INTERIOR = 0, CFD_FACE_WALL = 1, CFD_FACE_FARFIELD = 2, CFD_FACE_OUTLET = 3,
+       CFD_FACE_WAKECUT = 4 };
+
+/* A structured face-based mesh, as cfd::mesh::Mesh exposes it (Mesh.hpp:121-190).
+ * The arrays are read during cfd_gpu_create only and may be freed after it. */
+typedef struct cfd_mesh_desc {
+  int nodes_i, nodes_j;          /* Mesh::nodesI/nodesJ; cells = (ni-1)*(nj-1) */
+  int cell_count, face_count;
+  const double* cell_centroids;  /* 2*cells */
+  const double* cell_areas;      /* cells */
+  const double* face_centres;    /* 2*faces */
+  const double* face_normals;    /* 2*faces, unit, out of the owner */
+  const double* face_areas;      /* faces */
+  const int* face_owner;         /* faces */
+  const int* face_neighbour;     /* faces, -1 on a boundary */
+  const int* face_boundary;      /* faces, CFD_FACE_* */
+  const int* face_partner;       /* faces, wake-cut partner face or -1 */
+} cfd_mesh_desc;
+
+/* flow::FaceCondition per face (BoundaryConditions.hpp:101-107). */
+typedef struct cfd_face_bc {
+  const int* kind;         /* faces, CFD_BC_* */
+  const double* velocity;  /* 2*faces */
+  const double* pressure;  /* faces */
+} cfd_face_bc;
+
+/* solver::SimpleSettings (SimpleSolver.hpp:86-132) plus the precision form. */
+typedef struct cfd_settings {
+  double velocity_relaxation;      /* 0.5 */
+  double pressure_relaxation;      /* 0.2 */
+  int momentum_sweeps;             /* 3 */
+  int pressure_iterations;         /* 200 */
+  double pressure_tolerance;       /* 0.01 */
+  int scheme;                      /* 0 upwind, 1 second-order upwind */
+  double turbulence_relaxation;    /* 0.5 */
+  double inflow_intensity;         /* 0.001 (TurbulenceInflow) */
+  double inflow_viscosity_ratio;   /* 1.0 */
+  double inflow_length_scale;      /* 0.0 */
+  int non_orthogonal_correctors;   /* 1 */
+  double non_orthogonal_blend;     /* 1.0 */
+  int precision;                   /* 0 plain FP64 (the drop-in), 1 mixed FP32/FP64 */
+} cfd_settings;
+
+/* solver::SolverMonitor (SimpleSolver.hpp:135-154), flattened; plus the
+ * model's maxWallYPlus (TurbulenceModel.hpp:205). */
+typedef struct cfd_monitor {
+  double continuity, momentum_x, momentum_y;
+  double mass_imbalance, max_divergence;
+  int pressure_iterations;
+  int pad_;
+  double turbulence_first, turbulence_second;
+  double min_energy, max_energy, min_dissipation, max_dissipation;
+  double min_eddy_viscosity, max_eddy_viscosity;
+  double max_eddy_viscosity_ratio;
+  double max_wall_yplus;
+} cfd_monitor;
+
+/* Fields readable with cfd_gpu_read_field. (F) marks a per-face array in
+ * reference face order; (2N) a Vec2 per cell; the rest are per cell. */
+enum {
+  CFD_FIELD_U = 0, CFD_FIELD_V, CFD_FIELD_P, CFD_FIELD_RHO, CFD_FIELD_MU_EFF,
+  CFD_FIELD_MASS_FLUX /*F*/, CFD_FIELD_DIVERGENCE, CFD_FIELD_MU_MOLECULAR,
+  CFD_FIELD_GRAD_U /*2N*/, CFD_FIELD_GRAD_V /*2N*/, CFD_FIELD_GRAD_P /*2N*/,
+  CFD_FIELD_MOM_DIAG, CFD_FIELD_MOM_SOURCE_U, CFD_FIELD_MOM_SOURCE_V,
+  CFD_FIELD_MOM_UPPER /*F*/, CFD_FIELD_MOM_LOWER /*F*/, CFD_FIELD_MOMENTUM_DIAGONAL,
+  CFD_FIELD_P_DIAG, CFD_FIELD_P_SOURCE, CFD_FIELD_P_UPPER /*F*/, CFD_FIELD_NET_FLUX,
+  CFD_FIELD_P_CORRECTION,
+  CFD_FIELD_K, CFD_FIELD_OMEGA, CFD_FIELD_MUT, CFD_FIELD_WALL_DISTANCE, CFD_FIELD_STRAIN,
+  CFD_FIELD_F1, CFD_FIELD_F2, CFD_FIELD_CROSS_DIFFUSION, CFD_FIELD_PRODUCTION,
+  CFD_FIELD_GRAD_K /*2N*/, CFD_FIELD_GRAD_OMEGA /*2N*/,
+  CFD_FIELD_T_DIAG_K, CFD_FIELD_T_SOURCE_K, CFD_FIELD_T_DIAG_W, CFD_FIELD_T_SOURCE_W,
+  CFD_FIELD_COUNT
+};
+
+/* Stop points for cfd_gpu_iterate_partial: the iteration returns right after
+ * the named stage. The stage list follows SimpleSolver::iterate()
+ * (SimpleSolver.cpp:662-794) and KOmegaSST::update (KOmegaSST.cpp:531-548). */
+enum {
+  CFD_STAGE_GRADIENTS = 0,        /* interpolateFaceValues + computeGradients */
+  CFD_STAGE_MOMENTUM_ASSEMBLY,    /* assembleMomentum + applyRelaxation, u and v */
+  CFD_STAGE_MOMENTUM_SOLVE,       /* Gauss-Seidel sweeps */
+  CFD_STAGE_RHIE_CHOW,            /* computeRhieChowFluxes */
+  CFD_STAGE_PRESSURE_ASSEMBLY,    /* assemblePressureCorrection */
+  CFD_STAGE_PRESSURE_SOLVE,       /* conjugateGradient */
+  CFD_STAGE_CORRECT,              /* correct */
+  CFD_STAGE_SST_BLENDING,         /* computeStrain + computeBlending + production */
+  CFD_STAGE_SST_ASSEMBLY,         /* k and omega systems, relaxed */
+  CFD_STAGE_SST_SOLVE,            /* Gauss-Seidel sweeps (floors not yet applied) */
+  CFD_STAGE_END                   /* the whole iteration */
+};
+
+/* SimpleSolver::create (SimpleSolver.cpp:30-80): validates, copies the mesh
+ * metrics and face conditions to the device, precomputes face geometry.
+ * settings may be NULL for the reference defaults. */
+cfd_status cfd_gpu_create(const cfd_mesh_desc* mesh, const cfd_face_bc* conditions,
+                          const cfd_settings* settings, cfd_handle* out);
+
+/* SimpleSolver::setTurbulenceModel (SimpleSolver.cpp:212-230).
+ * model: 0 = none (nullptr), 1 = LaminarModel, 2 = KOmegaSST. */
+cfd_status cfd_gpu_set_turbulence(cfd_handle h, int model);
+
+/* SimpleSolver::initialise (SimpleSolver.cpp:133-210); arrays per cell. */
+cfd_status cfd_gpu_initialise(cfd_handle h, const double* u, const double* v, const double* p,
+                              const double* rho, const double* mu);
+
+/* n x SimpleSolver::iterate() (SimpleSolver.cpp:662-794) in one device launch.
+ * last (may be NULL) gets the final iteration's monitor, history (may be
+ * NULL) n monitors. Returns after the device has finished. */
+cfd_status cfd_gpu_iterate(cfd_handle h, int n, cfd_monitor* last, cfd_monitor* history);
+
+/* Iterate until worst() of the residuals < tol (SolverWorker.cpp:182-185),
+ * a non-finite residual, or cap iterations. Residuals are checked on the
+ * device every iteration; *taken gets the iterations run. */
+cfd_status cfd_gpu_converge(cfd_handle h, int cap, double tol, int* taken, cfd_monitor* last);
+
+/* One iteration stopped right after `stage` (CFD_STAGE_*): for stage-by-stage
+ * parity checks. The state afterwards is partial; re-load or re-initialise. */
+cfd_status cfd_gpu_iterate_partial(cfd_handle h, int stage, cfd_monitor* last);
+
+/* SimpleSolver::field()/massFlux()/divergence() and friends: copy one device
+ * field to host memory in reference order (see CFD_FIELD_*). */
+cfd_status cfd_gpu_read_field(cfd_handle h, int which, double* out);
+
+/* Overwrite the solver state (a warm start, or a state to continue from):
+ * u, v, p per cell; mass_flux per face (may be NULL to keep); k, omega, mut
+ * per cell (NULL unless SST); mu_eff per cell (may be NULL). */
+cfd_status cfd_gpu_load_state(cfd_handle h, const double* u, const double* v, const double* p,
+                              const double* mass_flux, const double* k, const double* omega,
+                              const double* mut, const double* mu_eff);
+
+/* SimpleSolver::setSettings (SimpleSolver.hpp:194). */
+cfd_status cfd_gpu_set_settings(cfd_handle h, const cfd_settings* settings);
+/* The reference defaults of SimpleSettings. */
+void cfd_default_settings(cfd_settings* out);
+
+/* Sizes: {cellsI, cellsJ, cells, faces}. */
+cfd_status cfd_gpu_dims(cfd_handle h, int* out4);
+/* SST freestream values {kInflow, omegaInflow}; referenceMassFlow. */
+cfd_status cfd_gpu_scalars(cfd_handle h, double* out3);
+
+cfd_status cfd_gpu_destroy(cfd_handle h);
+
+const char* cfd_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFD_GPU_H */

@@ -1,0 +1,107 @@
+"""Whole iterations and converged solves on the device, through the C ABI,
+against the CPU oracle and against the reference's converged answers
+(golden vectors). Tolerances are the parity contract: converged u, v, p, k,
+omega within 1e-9 relative L2 of the reference."""
+import numpy as np
+import pytest
+
+import cfd_b200 as cb
+from helpers import Case, golden, golden_mesh, rel_err, rel_l2
+from oracle import port
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["laminar_cgrid", "sst_cgrid", "sst_cambered"]
+CONVERGED_TOL = 1e-9
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_twenty_iterations_track_the_oracle(name):
+    c = Case(name)
+    o = c.oracle(port.RED_BLACK)
+    d = c.device()
+    mo = o.iterate(20)
+    last, hist = d.iterate(20, history=True)
+    assert np.all(np.isfinite(hist))
+    # monitors: same CG iteration counts to within one, residuals close
+    assert np.max(np.abs(hist[:, 5] - mo[:, 5])) <= 1
+    for field, fid in (("U", 0), ("V", 1), ("P", 2), ("MASS_FLUX", 5)):
+        assert rel_err(d.read(field), o.read(fid)) < 1e-7, field
+    if c.model == 2:
+        for field, fid in (("K", 22), ("OMEGA", 23), ("MUT", 24)):
+            assert rel_err(d.read(field), o.read(fid)) < 1e-7, field
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_converged_fields_match_the_reference(name):
+    c = Case(name)
+    g = c.g
+    d = c.device()
+    taken, mon = d.converge(20000, 1e-12 if c.model == 0 else 1e-11)
+    assert mon.worst() < (1e-12 if c.model == 0 else 1e-11), (taken, mon.worst())
+    fields = [("U", "u"), ("V", "v"), ("P", "p")]
+    if c.model == 2:
+        fields += [("K", "k"), ("OMEGA", "omega"), ("MUT", "mut")]
+    for field, key in fields:
+        err = rel_l2(d.read(field), g[f"converged/{key}"])
+        assert err < CONVERGED_TOL, (field, err)
+
+
+def test_laminar_closure_is_bit_identical_to_no_closure():
+    """TurbulenceTests.cpp:96-124: LaminarModel changes nothing."""
+    c = Case("laminar_cgrid")
+    a = c.device()
+    b = cb.SimpleSolver.create(c.mesh, c.conditions, c.settings())
+    b.set_turbulence_model(cb.MODEL_LAMINAR)
+    b.initialise(*c.initial)
+    a.iterate(15)
+    b.iterate(15)
+    for field in ("U", "V", "P", "MASS_FLUX", "MU_EFF"):
+        assert np.array_equal(a.read(field), b.read(field)), field
+
+
+def test_uniform_flow_is_reached_exactly():
+    """ValidationTests.cpp:98-139 on the device: a wrong uniform start reaches
+    the imposed stream to 1e-10 with max divergence < 1e-10."""
+    g = golden("box_cases")
+    mesh = cb.box(length=2.0, height=1.0, cells_x=20, cells_y=15, left=cb.FACE_FARFIELD,
+                  right=cb.FACE_OUTLET, lower=cb.FACE_FARFIELD, upper=cb.FACE_FARFIELD)
+    cond = cb.FaceConditions(g["uniform/kind"].astype(np.int32), g["uniform/velocity"],
+                             g["uniform/pressure"])
+    s = cb.SimpleSolver.create(mesh, cond, cb.Settings.defaults(velocity_relaxation=0.7,
+                                                               pressure_relaxation=0.3))
+    n = mesh.cells
+    s.initialise(np.full(n, 0.4), np.zeros(n), np.zeros(n), np.ones(n), np.full(n, 0.05))
+    taken, mon = s.converge(3000, 1e-12)
+    assert taken < 3000
+    assert np.max(np.abs(s.read("U") - 1.0)) < 1e-10
+    assert np.max(np.abs(s.read("V"))) < 1e-10
+    assert mon.max_divergence < 1e-10
+
+
+def test_channel_matches_the_reference():
+    """Plane channel (ValidationTests.cpp:203-275 set-up) against the
+    reference's converged fields."""
+    g = golden("box_cases")
+    mesh = cb.box(length=4.0, height=1.0, cells_x=24, cells_y=16, grading=2,
+                  first_cell_height=0.03)
+    cond = cb.FaceConditions(g["channel/kind"].astype(np.int32), g["channel/velocity"],
+                             g["channel/pressure"])
+    s = cb.SimpleSolver.create(mesh, cond, cb.Settings.defaults(velocity_relaxation=0.7,
+                                                               pressure_relaxation=0.3))
+    n = mesh.cells
+    s.initialise(np.ones(n), np.zeros(n), np.zeros(n), np.ones(n), np.full(n, 0.05))
+    taken, mon = s.converge(6000, 1e-11)
+    assert mon.worst() < 1e-11
+    for field, key in (("U", "u"), ("V", "v"), ("P", "p")):
+        assert rel_l2(s.read(field), g[f"channel/{key}"]) < CONVERGED_TOL, field
+
+
+def test_divergence_and_mass_flux_accessors():
+    c = Case("laminar_cgrid")
+    d = c.device()
+    d.iterate(3)
+    o = c.oracle(port.RED_BLACK)
+    o.iterate(3)
+    assert rel_err(d.divergence(), o.read(6)) < 1e-7
+    assert d.mass_flux().shape == (c.mesh.faces,)
