@@ -1,0 +1,383 @@
+"""Benchmark: steady SIMPLE (k-omega SST, plain FP64) on NACA 0012 C-grids.
+
+Workload (one "step" = one SIMPLE outer iteration of every solve in it):
+  NACA 0012, Re 1e6, k-omega SST, inflow intensity 0.1 %, mu_t/mu 10,
+  medium C-grid 384 x 96 cells (surface 128, wake 65, normal 97 points;
+  upstream/vertical 10 chords, downstream 15; first layer 1e-5 chord),
+  two solves at alpha 0 deg and 4 deg in one batched launch. Synthetic inputs:
+  the uniform freestream start of FlowField::uniform, advanced by the warm-up
+  steps; no dataset exists for this path.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is cell-iterations/s over all ranks,
+timed with CUDA events around each step's launch on the launching stream; L2
+(126 MB) is flushed between timed steps by writing a 256 MiB buffer. `e2e` is
+the same metric through the C ABI from pinned host buffers: each step loads
+the solver state host->device, iterates once, and reads the monitors back.
+`--impl reference` times the reference's own CPU solver (compiled from its
+sources into oracle/_ref) on the same workload with every host core.
+Multi-GPU (torchrun): independent replicas, one per GPU; no collective on the
+data path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "cfd-simulator_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "SIMPLE cell-iters/s, % HBM roofline; solves/min + p99, mixed vs FP64 at ΔCl≤1e-4"
+UNIT = "cell-iters/s"
+WORKLOAD = dict(designation="0012", surface_points=128, wake_points=65, normal_points=97,
+                first_layer_height=1e-5, upstream_chords=10.0, downstream_chords=15.0,
+                vertical_chords=10.0)
+ALPHAS = (0.0, 4.0)
+REYNOLDS = 1e6
+INTENSITY = 0.001
+VISCOSITY_RATIO = 10.0
+
+
+def config(extra=None):
+    c = {"workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 and 4 deg, "
+                     "plain FP64, batched in one launch",
+         "cells_per_solve": 384 * 96, "solves": len(ALPHAS), "model": "k-omega SST",
+         "precision": "fp64 plain (reference-parity form)",
+         "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------- clocks ---
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        mhz, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(mhz)) if mhz else None,
+                "sm_max_mhz": float(max(maxes)) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ---------------------------------------------------------------- workload ---
+
+def build_solvers(cb):
+    mesh = cb.cgrid(WORKLOAD["designation"], **{k: v for k, v in WORKLOAD.items() if k != "designation"})
+    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO)
+    solvers = []
+    for alpha in ALPHAS:
+        s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
+        s.set_turbulence_model(cb.MODEL_SST)
+        s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, REYNOLDS))
+        solvers.append(s)
+    return mesh, solvers
+
+
+def measured_peak() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic() -> dict | None:
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------- CPU leg ---
+
+def _ref_worker(args):
+    """One process: the reference solver (or the oracle port) on one solve,
+    `warm` untimed then `count` timed iterations. Returns (cells, seconds, kind)."""
+    alpha, warm, count = args
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, PKG)
+    from oracle import reference as R
+    w = WORKLOAD
+    settings = np.array([0.5, 0.2, 3, 200, 0.01, 0, 0.5, INTENSITY, VISCOSITY_RATIO, 0.0, 1, 1.0])
+    if R.available():
+        m = R.RefMesh.cgrid(w["designation"], w["surface_points"], w["wake_points"],
+                            w["normal_points"], w["first_layer_height"], w["upstream_chords"],
+                            w["downstream_chords"], w["vertical_chords"])
+        kind, vel, pres = m.conditions(1.0, alpha, 1.0, REYNOLDS)
+        s = R.RefSolver(m, kind, vel, pres, settings, turbulence=2)
+        s.initialise(*m.uniform(1.0, alpha, 1.0, REYNOLDS))
+        label = "reference"
+    else:
+        import cfd_b200 as cb
+        from oracle import port
+        m = cb.cgrid(w["designation"], **{k: v for k, v in w.items() if k != "designation"})
+        s = port.OracleSolver(m, cb.freestream_conditions(m, 1.0, alpha), settings, 2,
+                              port.LEXICOGRAPHIC)
+        s.initialise(*cb.uniform_field(m, 1.0, alpha, 1.0, REYNOLDS))
+        label = "port"
+    s.iterate(warm)
+    t0 = time.perf_counter()
+    s.iterate(count)
+    return m.cells, time.perf_counter() - t0, label
+
+
+def cpu_baseline(iterations: int = 60) -> dict:
+    """The reference CPU solver on one core: a bounded sample of the workload
+    (one of its solves, `iterations` outer iterations after 3 warm-up)."""
+    cells, seconds, kind = _ref_worker((ALPHAS[-1], 3, iterations))
+    return {"value": cells * iterations / seconds, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{iterations} SIMPLE iterations of one 384x96 SST solve (alpha {ALPHAS[-1]}), "
+                      f"single thread, {seconds:.1f} s"}
+
+
+def run_reference_arm(args) -> None:
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    procs = max(1, min(cores, 64))
+    per_step = 1
+    count = max(1, args.steps) * per_step
+    jobs = [(ALPHAS[k % len(ALPHAS)], args.warmup, count) for k in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        results = pool.map(_ref_worker, jobs)
+    wall = time.perf_counter() - t0
+    cells = sum(r[0] for r in results)
+    slowest = max(r[1] for r in results)
+    value = cells * count / slowest
+    kind = results[0][2]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": slowest / count * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config({"processes": procs}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+                         "sample": f"{procs} independent solves (alpha {ALPHAS}) x {count} timed "
+                                   f"iterations after {args.warmup} warm-up, one process per core; "
+                                   f"wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------- GPU arm ---
+
+def run_ours(args) -> None:
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+
+    import cfd_b200 as cb
+    cb.set_device(torch.cuda.current_device())
+    mesh, solvers = build_solvers(cb)
+    batch = cb.Batch(solvers)
+    cells = mesh.cells * len(solvers)
+    stream = torch.cuda.current_stream()
+    handle = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # warm-up (untimed), also moves the flow off its uniform start
+    for _ in range(args.warmup):
+        flush.zero_()
+        batch.launch(1, handle)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            batch.launch(1, handle)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    total_s = float(step_ms.sum()) / 1e3
+    gpu_launches = args.steps
+    _, monitors = batch.monitors()
+    finite = all(math.isfinite(m.continuity) for m in monitors)
+
+    # mean executed CG iterations: 20 more iterations with history
+    cg = []
+    for s in solvers:
+        _, hist = s.iterate(20, history=True)
+        cg.extend(hist[:, 5].tolist())
+    mean_cg = float(np.mean(cg))
+
+    # e2e through the C ABI from pinned host buffers
+    e2e_steps = max(5, min(50, args.steps))
+    states = []
+    for s in solvers:
+        arrays = {}
+        for name in ("U", "V", "P", "K", "OMEGA", "MUT", "MU_EFF"):
+            t = torch.empty(mesh.cells, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = s.read(name)
+            arrays[name] = t
+        t = torch.empty(mesh.faces, dtype=torch.float64, pin_memory=True)
+        t.numpy()[:] = s.read("MASS_FLUX")
+        arrays["MASS_FLUX"] = t
+        states.append(arrays)
+    h2d = sum(sum(t.numel() * 8 for t in a.values()) for a in states)
+    d2h = len(solvers) * 136
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        for s, a in zip(solvers, states):
+            s.load_state(u=a["U"].numpy(), v=a["V"].numpy(), p=a["P"].numpy(),
+                         mass_flux=a["MASS_FLUX"].numpy(), k=a["K"].numpy(),
+                         omega=a["OMEGA"].numpy(), mut=a["MUT"].numpy(), mu_eff=a["MU_EFF"].numpy())
+        taken, mons = batch.iterate(1)
+        assert all(t == 1 for t in taken)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+
+    # multi-rank: max time over ranks, cells summed
+    totals = np.array([total_s, e2e_s, cells], dtype=np.float64)
+    if dist is not None:
+        t = torch.tensor(totals[:2], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        c = torch.tensor([cells], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        total_s, e2e_s = (float(x) for x in t.tolist())
+        all_cells = float(c.item())
+    else:
+        all_cells = float(cells)
+    value = all_cells * args.steps / total_s
+    e2e_value = all_cells * e2e_steps / e2e_s
+
+    if rank == 0:
+        import bytes_model
+        peak, peak_kind = measured_peak()
+        per_launch_bytes = bytes_model.bytes_per_cell_iteration(True, mean_cg) * cells
+        mean_launch_s = float(np.mean(step_ms)) / 1e3
+        achieved = per_launch_bytes / mean_launch_s / 1e9
+        traffic = committed_traffic()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                    "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                    "kernel": "simpleKernel", "bytes_per_launch_algorithmic": per_launch_bytes,
+                    "mean_cg_iterations": mean_cg}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config({"cluster_shape": list(batch.shape())}),
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": gpu_launches, "clocks": clocks.summary(),
+            "finite": finite,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for s in solvers:
+        s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -153,6 +153,7 @@ def _sig(name, restype, *argtypes):
 _P = C.c_void_p
 _sig("cfd_last_error", C.c_char_p)
 _sig("cfd_default_settings", None, _P)
+_sig("cfd_set_device", C.c_int, C.c_int)
 _sig("cfd_gpu_create", C.c_int, _P, _P, _P, _P)
 _sig("cfd_gpu_set_turbulence", C.c_int, _P, C.c_int)
 _sig("cfd_gpu_initialise", C.c_int, _P, _P, _P, _P, _P, _P)
@@ -173,6 +174,12 @@ _sig("cfd_mesh_describe", C.c_int, _P, _P)
 _sig("cfd_mesh_nodes", _P, _P)
 _sig("cfd_mesh_face_conditions", C.c_int, _P, C.c_double, C.c_double, _P, _P, _P)
 _sig("cfd_mesh_free", None, _P)
+_sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
+_sig("cfd_batch_iterate", C.c_int, _P, C.c_int, C.c_double, _P, _P)
+_sig("cfd_batch_launch", C.c_int, _P, C.c_int, _P)
+_sig("cfd_batch_monitors", C.c_int, _P, _P, _P)
+_sig("cfd_batch_shape", C.c_int, _P, _P, _P)
+_sig("cfd_batch_destroy", C.c_int, _P)
 
 
 def _ptr(a: np.ndarray | None):
@@ -410,6 +417,55 @@ class SimpleSolver:
 
     def divergence(self) -> np.ndarray:
         return self.read("DIVERGENCE")
+
+
+def set_device(device: int) -> None:
+    """Select the CUDA device later solves are created on (this thread)."""
+    _check(_lib.cfd_set_device(device))
+
+
+class Batch:
+    """Many solves in one launch, one thread-block cluster each (cfd_batch_*)."""
+
+    def __init__(self, solvers: list[SimpleSolver]):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
+        self._h = C.c_void_p()
+        _check(_lib.cfd_batch_create(arr, len(self.solvers), C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.cfd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def iterate(self, n: int, tol: float = -1.0):
+        count = len(self.solvers)
+        taken = (C.c_int * count)()
+        last = (Monitor * count)()
+        _check(_lib.cfd_batch_iterate(self._h, n, tol, taken, last))
+        return list(taken), list(last)
+
+    def launch(self, n: int, stream: int | None = None) -> None:
+        """Enqueue n iterations on a CUDA stream (an int handle) without waiting."""
+        _check(_lib.cfd_batch_launch(self._h, n, None if stream is None else C.c_void_p(stream)))
+
+    def monitors(self):
+        count = len(self.solvers)
+        taken = (C.c_int * count)()
+        last = (Monitor * count)()
+        _check(_lib.cfd_batch_monitors(self._h, taken, last))
+        return list(taken), list(last)
+
+    def shape(self) -> tuple[int, int]:
+        cluster, threads = C.c_int(), C.c_int()
+        _check(_lib.cfd_batch_shape(self._h, C.byref(cluster), C.byref(threads)))
+        return cluster.value, threads.value
 
 
 def library_symbols() -> list[str]:

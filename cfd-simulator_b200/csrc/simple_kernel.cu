@@ -430,6 +430,58 @@ DEV void gsColour(const Instance& I, Team& t, int colour, const double* D, const
   }
 }
 
+/// Lexicographic Gauss-Seidel, executed as wavefronts: cells with i + j = d
+/// for d = 0, 1, ... Within a wavefront no cell depends on another; every
+/// cell sees its S and W neighbours already updated and its N and E
+/// neighbours not yet, exactly as in cell-index order. Across the wake cut,
+/// the partner (NI-1-i, 0) of (i, 0) lies on an earlier wavefront exactly when
+/// its cell index is smaller, so that coupling is reproduced too. The result
+/// is the reference's sweep (LinearSystem.cpp:77-116) to the last bit.
+///
+/// One CTA runs one system: rank 0 sweeps x1, rank 1 (or rank 0 again when
+/// the cluster has one CTA) sweeps x2. The caller ends with a cluster barrier.
+DEV void gsWavefrontSweeps(const Instance& I, Team& t, int sweeps, const double* D,
+                           const double* cS, const double* cN, const double* cW,
+                           const double* cE, const double* b1, double* x1, const double* D2,
+                           const double* cS2, const double* cN2, const double* cW2,
+                           const double* cE2, const double* b2, double* x2) {
+  const bool one = (t.R == 1);
+  if (!one && t.rank > 1) return;
+  const int fronts = I.NI + I.NJ - 1;
+  for (int sweep = 0; sweep < sweeps; ++sweep) {
+    for (int d = 0; d < fronts; ++d) {
+      const int jLo = (d - (I.NI - 1) > 0) ? d - (I.NI - 1) : 0;
+      const int jHi = (d < I.NJ - 1) ? d : I.NJ - 1;
+      const int count = jHi - jLo + 1;
+      const int work = one ? 2 * count : count;
+      for (int k = t.tid; k < work; k += t.T) {
+        const bool second = one ? (k >= count) : (t.rank == 1);
+        const int j = jLo + (one ? (k % count) : k);
+        const int i = d - j;
+        const int c = j * I.NI + i;
+        const double* Dv = second ? D2 : D;
+        const double dd = Dv[c];
+        if (!(fabs(dd) > 0.0)) continue;
+        const double* aS = second ? cS2 : cS;
+        const double* aN = second ? cN2 : cN;
+        const double* aW = second ? cW2 : cW;
+        const double* aE = second ? cE2 : cE;
+        double* x = second ? x2 : x1;
+        const double* b = second ? b2 : b1;
+        const int nS = across(I, c, i, j, 0), nE = across(I, c, i, j, 3);
+        const int nN = across(I, c, i, j, 1), nW = across(I, c, i, j, 2);
+        double off = 0.0;
+        if (nS >= 0) off += aS[c] * x[nS];
+        if (nE >= 0) off += aE[c] * x[nE];
+        if (nN >= 0) off += aN[c] * x[nN];
+        if (nW >= 0) off += aW[c] * x[nW];
+        x[c] = (b[c] - off) / dd;
+      }
+      __syncthreads();
+    }
+  }
+}
+
 // ---- phase: Rhie-Chow face fluxes (SimpleSolver.cpp:445-496) -------------------
 
 DEV void rhieChowFace(const Instance& I, const Face& f) {
@@ -1017,13 +1069,12 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       mon[kMonTurbSecond] = a4[2] / smax(a4[3] * smax(I.wIn, kTinySst), kTinySst);
       if (stopStage == kStageSstAssembly) { done = it + 1; break; }
 
-      for (int sweep = 0; sweep < 3; ++sweep) {
-        for (int colour = 0; colour < 2; ++colour) {
-          gsColour(I, t, colour, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN, I.wW,
-                   I.wE, I.wB, I.om);
-          t.cl.sync();
-        }
-      }
+      // k and omega sweep in the reference's cell order: their floors and
+      // the wall-cell omega override act after the sweeps, so the converged
+      // state depends on the order (a colouring would move it by ~1e-3).
+      gsWavefrontSweeps(I, t, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN, I.wW,
+                        I.wE, I.wB, I.om);
+      t.cl.sync();
       if (stopStage == kStageSstSolve) { done = it + 1; break; }
 
       double m8[8];

@@ -680,8 +680,7 @@ Status Solver::readField(int which, double* out) {
       // SimpleSolver::divergence (SimpleSolver.cpp:796-817), on the host.
       std::vector<double> flux(F), rho(N);
       Status st = CFD_OK;
-      if ((st = faces(I.mfN, I.mfE)) != CFD_OK) return st;
-      std::copy(out, out + F, flux.begin());
+      if ((st = readField(CFD_FIELD_MASS_FLUX, flux.data())) != CFD_OK) return st;
       if ((st = download(I.rho, N, rho.data())) != CFD_OK) return st;
       std::fill(out, out + N, 0.0);
       for (std::size_t f = 0; f < F; ++f) {
@@ -791,6 +790,12 @@ extern "C" {
 
 const char* cfd_last_error(void) { return cfdb::g_message.c_str(); }
 
+cfd_status cfd_set_device(int device) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INVALID_ARGUMENT, cudaGetErrorString(e));
+  return CFD_OK;
+}
+
 void cfd_default_settings(cfd_settings* out) {
   if (out != nullptr) cfdb::toC(cfdb::Settings{}, out);
 }
@@ -892,6 +897,137 @@ cfd_status cfd_gpu_destroy(cfd_handle h) {
   if (h == nullptr) return CFD_OK;
   delete h->solver;
   delete h;
+  return CFD_OK;
+}
+
+}  // extern "C"
+
+// ---- batches ------------------------------------------------------------------------------
+
+struct cfd_batch_t {
+  std::vector<cfd_handle> handles;
+  cfdb::Instance* dTable{nullptr};
+  cudaStream_t stream{nullptr};
+  int clusterSize{1};
+  int threads{512};
+  int lastIterations{0};
+};
+
+namespace {
+cfd_status refreshTable(cfd_batch b) {
+  std::vector<cfdb::Instance> table;
+  table.reserve(b->handles.size());
+  for (cfd_handle h : b->handles) table.push_back(h->solver->deviceView());
+  cudaError_t e = cudaMemcpyAsync(b->dTable, table.data(), table.size() * sizeof(cfdb::Instance),
+                                  cudaMemcpyHostToDevice, b->stream);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  return CFD_OK;
+}
+}  // namespace
+
+extern "C" {
+
+cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out) {
+  if (solvers == nullptr || out == nullptr || count <= 0) {
+    return cfdb::fail(CFD_INVALID_ARGUMENT, "a batch needs at least one solver");
+  }
+  auto* b = new cfd_batch_t;
+  for (int k = 0; k < count; ++k) {
+    if (solvers[k] == nullptr || solvers[k]->solver == nullptr) {
+      delete b;
+      return cfdb::fail(CFD_INVALID_ARGUMENT, "null solver in batch");
+    }
+    b->handles.push_back(solvers[k]);
+    b->clusterSize = std::max(b->clusterSize, solvers[k]->solver->clusterSize());
+  }
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dTable), count * sizeof(cfdb::Instance));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    if (b->dTable) cudaFree(b->dTable);
+    delete b;
+    return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  }
+  *out = b;
+  return refreshTable(b);
+}
+
+cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream) {
+  if (b == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null batch");
+  if (n < 1 || n > 256) return cfdb::fail(CFD_OUT_OF_RANGE, "a batch launch runs 1 to 256 iterations");
+  for (cfd_handle h : b->handles) {
+    if (!h->solver->initialised()) return cfdb::fail(CFD_INVALID_ARGUMENT, "a solver in the batch is not initialised");
+  }
+  cudaStream_t s = (stream != nullptr) ? static_cast<cudaStream_t>(stream) : b->stream;
+  b->lastIterations = n;
+  return cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize, b->threads, n,
+                            cfdb::kStageEnd, -1.0, s);
+}
+
+cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last) {
+  if (b == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null batch");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  for (std::size_t k = 0; k < b->handles.size(); ++k) {
+    const cfdb::Instance& I = b->handles[k]->solver->deviceView();
+    int ran = 0;
+    e = cudaMemcpy(&ran, I.iterations, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    if (taken != nullptr) taken[k] = ran;
+    if (last != nullptr && ran > 0) {
+      double h[cfdb::kMonSlots];
+      e = cudaMemcpy(h, I.history + static_cast<std::size_t>(ran - 1) * cfdb::kMonSlots, sizeof(h),
+                     cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+      packMonitor(h, last + k);
+    }
+  }
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_monitor* last) {
+  if (b == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null batch");
+  if (cfd_status st = refreshTable(b); st != CFD_OK) return st;
+  int done = 0;
+  std::vector<int> total(b->handles.size(), 0);
+  std::vector<int> ran(b->handles.size(), 0);
+  while (done < n) {
+    const int chunk = std::min(n - done, 256);
+    for (cfd_handle h : b->handles) {
+      if (!h->solver->initialised()) return cfdb::fail(CFD_INVALID_ARGUMENT, "a solver in the batch is not initialised");
+    }
+    if (cfd_status st = cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize,
+                                           b->threads, chunk, cfdb::kStageEnd, tol, b->stream);
+        st != CFD_OK) {
+      return st;
+    }
+    if (cfd_status st = cfd_batch_monitors(b, ran.data(), last); st != CFD_OK) return st;
+    bool allStopped = true;
+    for (std::size_t k = 0; k < ran.size(); ++k) {
+      total[k] += ran[k];
+      if (ran[k] == chunk) allStopped = false;
+    }
+    done += chunk;
+    if (tol >= 0.0 && allStopped) break;
+  }
+  if (taken != nullptr) std::copy(total.begin(), total.end(), taken);
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_shape(cfd_batch b, int* clusterSize, int* threads) {
+  if (b == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null batch");
+  if (clusterSize != nullptr) *clusterSize = b->clusterSize;
+  if (threads != nullptr) *threads = b->threads;
+  return CFD_OK;
+}
+
+cfd_status cfd_batch_destroy(cfd_batch b) {
+  if (b == nullptr) return CFD_OK;
+  cudaStreamSynchronize(b->stream);
+  cudaFree(b->dTable);
+  cudaStreamDestroy(b->stream);
+  delete b;
   return CFD_OK;
 }
 

@@ -87,6 +87,7 @@ class Solver {
   double omegaInflow() const { return wIn_; }
   double referenceMassFlow() const { return refMassFlow_; }
   int clusterSize() const { return clusterSize_; }
+  bool initialised() const { return initialised_; }
   const Instance& deviceView() const { return view_; }
   cudaStream_t stream() const { return stream_; }
 

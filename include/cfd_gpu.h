@@ -188,6 +188,34 @@ cfd_status cfd_gpu_destroy(cfd_handle h);
 
 const char* cfd_last_error(void);
 
+/* Make `device` the CUDA device this thread's later calls create solves on
+ * (one process per GPU: each rank selects its own). No reference
+ * counterpart: the reference has no device. */
+cfd_status cfd_set_device(int device);
+
+/* ---- batches: many solves in one launch ------------------------------------
+ * A batch is a descriptor table over existing handles (each keeps its own
+ * device state). One launch runs every solve of the table, one thread-block
+ * cluster each, so uneven sizes, angles and sections share the GPU. The
+ * reference runs one solve per worker thread (src/app/SolverWorker.cpp); this
+ * has no counterpart there. The handles must outlive the batch and must not
+ * be iterated on their own while a batch launch is in flight. */
+typedef struct cfd_batch_t* cfd_batch;
+
+cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out);
+/* n iterations of every solve; tol >= 0 lets each solve stop on its own at
+ * convergence or divergence. taken (may be NULL) gets count iteration counts,
+ * last (may be NULL) count monitors. Synchronous. */
+cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_monitor* last);
+/* Enqueue n iterations on `stream` (a cudaStream_t; NULL for the batch's own
+ * stream) and return without waiting; for callers that time with events. */
+cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream);
+/* Monitors of the last launch (count entries); synchronises first. */
+cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last);
+/* Cluster size (CTAs per solve) and threads per CTA used by launches. */
+cfd_status cfd_batch_shape(cfd_batch b, int* cluster_size, int* threads);
+cfd_status cfd_batch_destroy(cfd_batch b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -868,8 +868,8 @@ static int iterate_once(or_solver* s, int stop, double* mon) {
   memcpy(s->momDiag, s->mom.diag, sizeof(double) * N);
   if (stop == ST_MOM_ASSEMBLY) { free(scratch); return 1; }
 
-  gauss_seidel(m, s->cellFaces, s->mom.diag, s->mom.source, s->mom.upper, s->mom.lower, s->u, s->sweeps, s->gsOrder);
-  gauss_seidel(m, s->cellFaces, s->mom.diag, s->srcV, s->mom.upper, s->mom.lower, s->v, s->sweeps, s->gsOrder);
+  gauss_seidel(m, s->cellFaces, s->mom.diag, s->mom.source, s->mom.upper, s->mom.lower, s->u, s->sweeps, s->gsOrder & 1);
+  gauss_seidel(m, s->cellFaces, s->mom.diag, s->srcV, s->mom.upper, s->mom.lower, s->v, s->sweeps, s->gsOrder & 1);
   if (stop == ST_MOM_SOLVE) { free(scratch); return 1; }
 
   rhie_chow(s);
@@ -910,8 +910,8 @@ static int iterate_once(or_solver* s, int stop, double* mon) {
     sst_assemble_both(s);
     mon[6] = s->resK; mon[7] = s->resW;
     if (stop == ST_SST_ASSEMBLY) return 1;
-    gauss_seidel(m, s->cellFaces, s->tk.diag, s->tk.source, s->tk.upper, s->tk.lower, s->k, 3, s->gsOrder);
-    gauss_seidel(m, s->cellFaces, s->tw.diag, s->tw.source, s->tw.upper, s->tw.lower, s->om, 3, s->gsOrder);
+    gauss_seidel(m, s->cellFaces, s->tk.diag, s->tk.source, s->tk.upper, s->tk.lower, s->k, 3, (s->gsOrder >> 1) & 1);
+    gauss_seidel(m, s->cellFaces, s->tw.diag, s->tw.source, s->tw.upper, s->tw.lower, s->om, 3, (s->gsOrder >> 1) & 1);
     if (stop == ST_SST_SOLVE) return 1;
     sst_finish(s, mon);
   } else if (s->model == 1) {

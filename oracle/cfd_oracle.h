@@ -35,9 +35,10 @@ typedef struct or_solver or_solver;
 
 /* settings: the 12 SimpleSettings values {alphaU, alphaP, sweeps, cgMax,
  * cgTol, scheme, alphaT, intensity, viscosityRatio, lengthScale, nCorr,
- * blend}. model: 0 none, 1 laminar closure, 2 SST. gs_order: 0 lexicographic
- * (the reference), 1 red-black (the device solver). The mesh arrays must
- * outlive the solver. NULL on invalid input (or_last_error()). */
+ * blend}. model: 0 none, 1 laminar closure, 2 SST. gs_order is a bit mask:
+ * bit 0 sweeps the momentum equations red-black, bit 1 the k and omega
+ * equations; 0 is the reference (all lexicographic), 1 the device solver.
+ * The mesh arrays must outlive the solver. NULL on invalid input. */
 or_solver* or_create(const or_mesh* mesh, const int* kind, const double* velocity,
                      const double* pressure, const double* settings, int model, int gs_order);
 int or_initialise(or_solver* s, const double* u, const double* v, const double* p,
@@ -57,7 +58,8 @@ void or_scalars(or_solver* s, double* out3);
 void or_free(or_solver* s);
 const char* or_last_error(void);
 
-/* LDU primitives (LinearSystem.cpp), on the same mesh layout. */
+/* LDU primitives (LinearSystem.cpp), on the same mesh layout; gs_order 0
+ * lexicographic, 1 red-black. */
 void or_ldu_multiply(const or_mesh* m, const double* diag, const double* upper,
                      const double* lower, const double* x, double* y);
 void or_ldu_gauss_seidel(const or_mesh* m, const double* diag, const double* source,

@@ -68,14 +68,18 @@ def mesh_struct(mesh) -> OrMesh:
 FACE_FIELDS = {5, 14, 15, 19}
 VEC2_FIELDS = {8, 9, 10, 31, 32}
 
-LEXICOGRAPHIC, RED_BLACK = 0, 1
+# Gauss-Seidel orders (bit 0: momentum red-black, bit 1: k and omega red-black)
+LEXICOGRAPHIC = 0   # the reference
+DEVICE_ORDER = 1    # the device solver: momentum red-black, k and omega lexicographic
+RED_BLACK = 1       # for the LDU primitive: red-black
+RED_BLACK_ALL = 3
 
 
 class OracleSolver:
     """The restated SIMPLE solve, on a mesh held by the caller."""
 
     def __init__(self, mesh, conditions, settings_packed: np.ndarray, model: int = 0,
-                 gs_order: int = RED_BLACK):
+                 gs_order: int = DEVICE_ORDER):
         self.mesh = mesh
         self._m = mesh_struct(mesh)
         self._keep = (conditions.kind, conditions.velocity, conditions.pressure,

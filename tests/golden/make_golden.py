@@ -131,12 +131,17 @@ def make_case(name: str) -> None:
         out[f"iter5/{key}"] = s.read(fid)
     del s
 
-    # Converged: the SolverWorker stop rule at a tight tolerance.
+    # Converged: the SolverWorker stop rule at a tight tolerance, then 2000
+    # more iterations. The stop rule reads only the flow residuals; k and
+    # omega keep settling for a while after it fires, so the fixed point is
+    # taken from the settled state.
     s = R.RefSolver(m, kind, vel, pres, settings, turbulence=model)
     s.initialise(u, v, p, rho, mu)
     taken, mon = s.converge(40000, 1e-12 if model == 0 else 1e-11)
-    out["converged/iterations"] = np.int32(taken)
-    out["converged/monitor"] = mon
+    settle = s.iterate(2000)
+    out["converged/stop_rule_iterations"] = np.int32(taken)
+    out["converged/iterations"] = np.int32(taken + 2000)
+    out["converged/monitor"] = settle[-1]
     for key, fid in fields + (sst_fields[:3] if model == 2 else []):
         out[f"converged/{key}"] = s.read(fid)
     forces, cp = s.forces(1.0, alpha, 1.0, re)

@@ -52,7 +52,7 @@ class Case:
             inflow_length_scale=p[9], non_orthogonal_correctors=int(p[10]),
             non_orthogonal_blend=p[11])
 
-    def oracle(self, gs_order=port.RED_BLACK) -> port.OracleSolver:
+    def oracle(self, gs_order=port.DEVICE_ORDER) -> port.OracleSolver:
         s = port.OracleSolver(self.mesh, self.conditions, self.packed, self.model, gs_order)
         s.initialise(*self.initial)
         return s
