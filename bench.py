@@ -249,8 +249,12 @@ def run_ours(args) -> None:
     mesh, solvers = build_solvers(cb)
     batch = cb.Batch(solvers)
     cells = mesh.cells * len(solvers)
-    stream = torch.cuda.current_stream()
+    # A stream of our own: events, the L2 flush and the solver launches all go
+    # on it (torch's default stream is the legacy NULL stream, handle 0).
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     handle = stream.cuda_stream
+    assert handle != 0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     # warm-up (untimed), also moves the flow off its uniform start

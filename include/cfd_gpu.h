@@ -207,8 +207,9 @@ cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out
  * convergence or divergence. taken (may be NULL) gets count iteration counts,
  * last (may be NULL) count monitors. Synchronous. */
 cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_monitor* last);
-/* Enqueue n iterations on `stream` (a cudaStream_t; NULL for the batch's own
- * stream) and return without waiting; for callers that time with events. */
+/* Enqueue n iterations on `stream` (a cudaStream_t; NULL means the batch's
+ * own stream, not the legacy default stream) and return without waiting;
+ * for callers that time with events on their own stream. */
 cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream);
 /* Monitors of the last launch (count entries); synchronises first. */
 cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last);
