@@ -141,13 +141,18 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def committed_traffic() -> dict | None:
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def committed_traffic() -> float | None:
+    """DRAM bytes per launch of simpleKernel on this workload, from the
+    committed ncu summary (its `traffic_bytes_per_launch:` line)."""
+    path = os.path.join(ROOT, "profiles", "simple_kernel_c2_sst_fp64.md")
     try:
         with open(path) as f:
-            return json.load(f)
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1])
     except (OSError, ValueError):
-        return None
+        pass
+    return None
 
 
 # ------------------------------------------------------------- CPU leg ---
@@ -342,7 +347,7 @@ def run_ours(args) -> None:
         traffic = committed_traffic()
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                    "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                    "traffic": traffic,
                     "kernel": "simpleKernel", "bytes_per_launch_algorithmic": per_launch_bytes,
                     "mean_cg_iterations": mean_cg}
         line = {

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -357,6 +358,16 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
   CUDA_OR_FAIL(cudaMemcpy(wallDist_.data(), I.wallDist, N * sizeof(double), cudaMemcpyDeviceToHost));
 
   clusterSize_ = chooseClusterSize(N_);
+  // Launch-shape overrides for tuning sweeps: CTAs per solve (1..16) and
+  // threads per CTA (a multiple of 32, at most 512).
+  if (const char* env = std::getenv("CFD_CLUSTER_SIZE")) {
+    const int r = std::atoi(env);
+    if (r >= 1 && r <= 16) clusterSize_ = r;
+  }
+  if (const char* env = std::getenv("CFD_THREADS")) {
+    const int t = std::atoi(env);
+    if (t >= 32 && t <= 512 && t % 32 == 0) threads_ = t;
+  }
   return uploadSettings();
 }
 
@@ -941,6 +952,7 @@ cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out
     }
     b->handles.push_back(solvers[k]);
     b->clusterSize = std::max(b->clusterSize, solvers[k]->solver->clusterSize());
+    b->threads = solvers[k]->solver->threads();
   }
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dTable), count * sizeof(cfdb::Instance));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);

@@ -88,6 +88,7 @@ class Solver {
   double referenceMassFlow() const { return refMassFlow_; }
   int clusterSize() const { return clusterSize_; }
   bool initialised() const { return initialised_; }
+  int threads() const { return threads_; }
   const Instance& deviceView() const { return view_; }
   cudaStream_t stream() const { return stream_; }
 
