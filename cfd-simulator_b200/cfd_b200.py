@@ -174,6 +174,7 @@ _sig("cfd_mesh_describe", C.c_int, _P, _P)
 _sig("cfd_mesh_nodes", _P, _P)
 _sig("cfd_mesh_face_conditions", C.c_int, _P, C.c_double, C.c_double, _P, _P, _P)
 _sig("cfd_mesh_free", None, _P)
+_sig("cfd_cg_solve", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
 _sig("cfd_batch_iterate", C.c_int, _P, C.c_int, C.c_double, _P, _P)
 _sig("cfd_batch_launch", C.c_int, _P, C.c_int, _P)
@@ -417,6 +418,23 @@ class SimpleSolver:
 
     def divergence(self) -> np.ndarray:
         return self.read("DIVERGENCE")
+
+
+class CgSystem(C.Structure):
+    """cfd_cg_system: device pointers of a symmetric five-point LDU system."""
+    _fields_ = [("cells_i", C.c_int), ("cells_j", C.c_int), ("diag", C.c_void_p),
+                ("upper", C.c_void_p), ("source", C.c_void_p), ("across_j0", C.c_void_p)]
+
+
+def cg_solve(system: CgSystem, x_ptr: int, tolerance: float, max_iterations: int,
+             stream: int | None = None) -> np.ndarray:
+    """conjugateGradient on the device (cfd_cg_solve); x_ptr is a device
+    pointer to the start vector, overwritten with the solution. Returns the
+    report {iterations, initial residual, final residual, converged}."""
+    report = np.zeros(4)
+    _check(_lib.cfd_cg_solve(C.byref(system), C.c_void_p(x_ptr), tolerance, max_iterations,
+                             _ptr(report), None if stream is None else C.c_void_p(stream)))
+    return report
 
 
 def set_device(device: int) -> None:

@@ -1,0 +1,261 @@
+// cg_solve.cu - the reference's Jacobi-preconditioned conjugate gradient
+// (LinearSystem.cpp:118-210) as a device primitive on one thread-block
+// cluster, for a symmetric five-point system on a structured block given in
+// the reference's LDU layout (LinearSystem.hpp:29-71).
+//
+// The iteration is the reference's, with its L1 stopping rule and its
+// breakdown guards; the dot products are summed in a fixed order (warp
+// trees, then CTA ranks in order), so a solve is deterministic. Two cluster
+// barriers per iteration: the next direction d' = z + beta d is formed for a
+// cell and, redundantly, for its neighbours from z and d, which are both
+// stable across the barrier.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+
+#include "cfd_gpu.h"
+#include "common.hpp"
+#include "solver.hpp"
+#include "team.cuh"
+
+namespace cfdb {
+
+/// A five-point symmetric system on an NI x NJ block, in the device layout:
+/// per-face coefficients in N-face (j*NI + i) and E-face (j*(NI+1) + i) order.
+struct CgView {
+  int NI, NJ, N;
+  const int* acrossJ0;
+  const double* diag;
+  const double* pN;
+  const double* pE;
+  const double* b;
+  double *x, *r, *z, *q, *d0, *d1;
+  int maxIt;
+  double tol;
+  double* report;  // {iterations, initial, final, converged}
+};
+
+namespace {
+
+DEV double rowTimes(const CgView& V, int c, int i, int j, const double* v, double vc) {
+  double y = V.diag[c] * vc;
+  if (j > 0) y += V.pN[j * V.NI + i] * v[c - V.NI];
+  else if (V.acrossJ0[i] >= 0) y += V.pN[i] * v[V.acrossJ0[i]];
+  if (j < V.NJ - 1) y += V.pN[(j + 1) * V.NI + i] * v[c + V.NI];
+  if (i > 0) y += V.pE[j * (V.NI + 1) + i] * v[c - 1];
+  if (i < V.NI - 1) y += V.pE[j * (V.NI + 1) + i + 1] * v[c + 1];
+  return y;
+}
+
+DEV double precondition(double rc, double dg) { return (fabs(dg) > 0.0) ? rc / dg : rc; }
+
+}  // namespace
+
+/// The whole solve, run by every thread of the cluster.
+__device__ void cgSolveTeam(const CgView& V, Team& t, Shared& sh) {
+  const int op2[2] = {kSum, kSum};
+  const int op1[1] = {kSum};
+  double init[2] = {0.0, 0.0};
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % V.NI, j = c / V.NI;
+    const double rc = V.b[c] - rowTimes(V, c, i, j, V.x, V.x[c]);
+    const double zc = precondition(rc, V.diag[c]);
+    V.r[c] = rc;
+    V.z[c] = zc;
+    V.d0[c] = zc;
+    init[0] += fabs(rc);
+    init[1] += rc * zc;
+  }
+  teamReduce(t, sh, init, op2);
+  const double initial = init[0];
+  double rz = init[1];
+  double finalResidual = initial;
+  int iterations = 0;
+  bool converged = false;
+  if (initial <= 0.0) {
+    converged = true;
+  } else {
+    double* dCur = V.d0;
+    double* dNext = V.d1;
+    double beta = 0.0;
+    for (int iter = 0; iter < V.maxIt; ++iter) {
+      double dAd[1] = {0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        const int i = c % V.NI, j = c / V.NI;
+        double dc;
+        if (iter == 0) {
+          dc = dCur[c];
+          V.q[c] = rowTimes(V, c, i, j, dCur, dc);
+        } else {
+          dc = V.z[c] + beta * dCur[c];
+          dNext[c] = dc;
+          double y = V.diag[c] * dc;
+          int n = (j > 0) ? c - V.NI : V.acrossJ0[i];
+          if (n >= 0) y += V.pN[j * V.NI + i] * (V.z[n] + beta * dCur[n]);
+          if (j < V.NJ - 1) { n = c + V.NI; y += V.pN[(j + 1) * V.NI + i] * (V.z[n] + beta * dCur[n]); }
+          if (i > 0) { n = c - 1; y += V.pE[j * (V.NI + 1) + i] * (V.z[n] + beta * dCur[n]); }
+          if (i < V.NI - 1) { n = c + 1; y += V.pE[j * (V.NI + 1) + i + 1] * (V.z[n] + beta * dCur[n]); }
+          V.q[c] = y;
+        }
+        dAd[0] += dc * V.q[c];
+      }
+      if (iter > 0) { double* tmp = dCur; dCur = dNext; dNext = tmp; }
+      teamReduce(t, sh, dAd, op1);
+      if (!(fabs(dAd[0]) > 0.0)) break;
+      const double step = rz / dAd[0];
+      double rr[2] = {0.0, 0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        V.x[c] += step * dCur[c];
+        const double rc = V.r[c] - step * V.q[c];
+        V.r[c] = rc;
+        const double zc = precondition(rc, V.diag[c]);
+        V.z[c] = zc;
+        rr[0] += fabs(rc);
+        rr[1] += rc * zc;
+      }
+      teamReduce(t, sh, rr, op2);
+      iterations = iter + 1;
+      finalResidual = rr[0];
+      if (rr[0] <= V.tol * initial) {
+        converged = true;
+        break;
+      }
+      if (!(fabs(rz) > 0.0)) break;
+      beta = rr[1] / rz;
+      rz = rr[1];
+    }
+  }
+  if (t.rank == 0 && t.tid == 0 && V.report != nullptr) {
+    V.report[0] = static_cast<double>(iterations);
+    V.report[1] = initial;
+    V.report[2] = finalResidual;
+    V.report[3] = converged ? 1.0 : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(512, 1) cgSolveKernel(CgView V) {
+  __shared__ Shared sh;
+  Team t{cg::this_cluster(), 0, 0, 0, 0, 0, 0, 0};
+  t.rank = t.cl.block_rank();
+  t.R = t.cl.num_blocks();
+  t.tid = threadIdx.x;
+  t.T = blockDim.x;
+  t.c0 = static_cast<int>((static_cast<long long>(V.N) * t.rank) / t.R);
+  t.c1 = static_cast<int>((static_cast<long long>(V.N) * (t.rank + 1)) / t.R);
+  cgSolveTeam(V, t, sh);
+  t.cl.sync();  // no CTA leaves while a peer may still read its shared memory
+}
+
+/// Reference-order face coefficients -> device layout; missing wake map -> -1.
+__global__ void cgLayoutKernel(int NI, int NJ, const double* upper, const int* across, double* pN,
+                               double* pE, int* acrossOut) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jFaces = NI * (NJ + 1);
+  const int faces = jFaces + (NI + 1) * NJ;
+  if (f < NI) acrossOut[f] = (across != nullptr) ? across[f] : -1;
+  if (f >= faces) return;
+  if (f < jFaces) {
+    pN[f] = upper[f];
+  } else {
+    const int g = f - jFaces, i = g / NJ, j = g % NJ;
+    pE[j * (NI + 1) + i] = upper[f];
+  }
+}
+
+/// Validate a system's sizes; fills the view's dimensions.
+Status cgCheck(const cfd_cg_system* s, const double* x, int maxIt, CgView* V) {
+  if (s == nullptr || x == nullptr || s->diag == nullptr || s->upper == nullptr ||
+      s->source == nullptr) {
+    return fail(CFD_INVALID_ARGUMENT, "null system array");
+  }
+  if (s->cells_i < 1 || s->cells_j < 1) return fail(CFD_INVALID_ARGUMENT, "empty block");
+  if (maxIt < 0) return fail(CFD_INVALID_ARGUMENT, "negative iteration cap");
+  const long long cells = static_cast<long long>(s->cells_i) * s->cells_j;
+  if (cells > (1LL << 30)) return fail(CFD_OUT_OF_RANGE, "block too large");
+  V->NI = s->cells_i;
+  V->NJ = s->cells_j;
+  V->N = static_cast<int>(cells);
+  return CFD_OK;
+}
+
+/// Lay out the coefficients, then solve on one cluster (two launches on `stream`).
+Status cgRun(const cfd_cg_system* s, CgView V, cudaStream_t stream) {
+  const int faces = V.NI * (V.NJ + 1) + (V.NI + 1) * V.NJ;
+  const int block = 256;
+  cgLayoutKernel<<<(faces + block - 1) / block, block, 0, stream>>>(
+      V.NI, V.NJ, s->upper, s->across_j0, const_cast<double*>(V.pN), const_cast<double*>(V.pE),
+      const_cast<int*>(V.acrossJ0));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  static bool configured = false;
+  if (!configured) {
+    e = cudaFuncSetAttribute(cgSolveKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    configured = true;
+  }
+  const int R = chooseClusterSize(V.N);
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(static_cast<unsigned>(R), 1, 1);
+  config.blockDim = dim3(512, 1, 1);
+  config.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = static_cast<unsigned>(R);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  config.attrs = attr;
+  config.numAttrs = 1;
+  e = cudaLaunchKernelEx(&config, cgSolveKernel, V);
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, std::string("CG launch: ") + cudaGetErrorString(e));
+  return CFD_OK;
+}
+
+}  // namespace cfdb
+
+extern "C" {
+
+cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance,
+                        int max_iterations, double* report, void* stream) {
+  cfdb::CgView V{};
+  if (cfd_status st = cfdb::cgCheck(system, x, max_iterations, &V); st != CFD_OK) return st;
+  const std::size_t N = V.N;
+  const std::size_t FN = static_cast<std::size_t>(V.NI) * (V.NJ + 1);
+  const std::size_t FE = static_cast<std::size_t>(V.NI + 1) * V.NJ;
+  // Scratch for this call: both coefficient families, five CG vectors, the
+  // wake map and the report.
+  const std::size_t doubles = FN + FE + 5 * N + 4;
+  char* scratch = nullptr;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&scratch), doubles * sizeof(double) + V.NI * sizeof(int));
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  double* p = reinterpret_cast<double*>(scratch);
+  V.pN = p; p += FN;
+  V.pE = p; p += FE;
+  V.r = p; p += N;
+  V.z = p; p += N;
+  V.q = p; p += N;
+  V.d0 = p; p += N;
+  V.d1 = p; p += N;
+  V.report = p; p += 4;
+  V.acrossJ0 = reinterpret_cast<const int*>(p);
+  V.diag = system->diag;
+  V.b = system->source;
+  V.x = x;
+  V.maxIt = max_iterations;
+  V.tol = tolerance;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cfd_status st = cfdb::cgRun(system, V, s);
+  if (st == CFD_OK) {
+    double host[4];
+    e = cudaMemcpyAsync(host, V.report, sizeof(host), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    else if (report != nullptr) for (int k = 0; k < 4; ++k) report[k] = host[k];
+  }
+  cudaFree(scratch);
+  return st;
+}
+
+}  // extern "C"

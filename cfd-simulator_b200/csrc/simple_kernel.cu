@@ -44,18 +44,12 @@
 #include "common.hpp"
 #include "instance.hpp"
 #include "solver.hpp"
-
-namespace cg = cooperative_groups;
+#include "team.cuh"
 
 namespace cfdb {
 namespace {
 
 #define DEV __device__ __forceinline__
-
-// std::max / std::min / std::clamp semantics, NaN behaviour included.
-DEV double smax(double a, double b) { return (a < b) ? b : a; }
-DEV double smin(double a, double b) { return (b < a) ? b : a; }
-DEV double sclamp(double v, double lo, double hi) { return (v < lo) ? lo : ((hi < v) ? hi : v); }
 
 constexpr double kTinySolver = 1e-300;  // SimpleSolver.cpp:16
 constexpr double kTinySst = 1.0e-30;    // KOmegaSST.cpp:22
@@ -67,78 +61,6 @@ constexpr double kBetaStar = 0.09, kKappa = 0.41, kA1 = 0.31, kProdLimit = 10.0;
 
 // BoundaryKind values (cfd_gpu.h).
 constexpr int kInternal = 0, kInlet = 1, kOutlet = 2, kFarField = 3, kWall = 4;
-
-constexpr int kMaxWarps = 32;
-constexpr int kRedSlots = 8;
-
-struct Shared {
-  double warp[kMaxWarps][kRedSlots];
-  double part[2][kRedSlots];
-  double result[kRedSlots];
-};
-
-struct Team {
-  cg::cluster_group cl;
-  unsigned rank, R;
-  int tid, T;
-  int c0, c1;
-  int buf;
-};
-
-// ---- reductions -------------------------------------------------------------
-
-enum RedOp : int { kSum = 0, kMax = 1 };
-
-DEV double combine(int op, double a, double b) { return (op == kMax) ? smax(a, b) : a + b; }
-DEV double identity(int op) { return (op == kMax) ? -INFINITY : 0.0; }
-
-/// Reduce K values over every thread of the cluster. The result is the same
-/// bits in every thread of every CTA. Contains a cluster barrier.
-template <int K>
-DEV void teamReduce(Team& t, Shared& sh, double (&v)[K], const int (&op)[K]) {
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwarps = (t.T + 31) >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      v[k] = combine(op[k], v[k], __shfl_down_sync(0xffffffffu, v[k], off));
-    }
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) sh.warp[warp][k] = v[k];
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double a = (lane < nwarps) ? sh.warp[lane][k] : identity(op[k]);
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
-      if (lane == 0) sh.part[t.buf][k] = a;
-    }
-  }
-  t.cl.sync();
-  if (warp == 0) {
-#pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double a = identity(op[k]);
-      if (lane < static_cast<int>(t.R)) {
-        const double* remote = t.cl.map_shared_rank(&sh.part[t.buf][k], lane);
-        a = *remote;
-      }
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
-      if (lane == 0) sh.result[k] = a;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < K; ++k) v[k] = sh.result[k];
-  t.buf ^= 1;
-}
 
 // ---- faces of a cell ----------------------------------------------------------
 

@@ -193,6 +193,31 @@ const char* cfd_last_error(void);
  * counterpart: the reference has no device. */
 cfd_status cfd_set_device(int device);
 
+/* ---- the pressure-correction CG as a device primitive -----------------------
+ * A symmetric five-point system on a structured block, in the layout of the
+ * reference's LinearSystem (LinearSystem.hpp:29-71): diag and source per cell,
+ * one off-diagonal per face in reference face order (upper; the solve uses it
+ * for both rows, so lower must equal it). A j = 0 face of column i couples to
+ * across_j0[i] when that is >= 0 (the wake cut; Mesh.cpp:78-87). Every
+ * pointer is device memory. */
+typedef struct cfd_cg_system {
+  int cells_i, cells_j;
+  const double* diag;     /* cells */
+  const double* upper;    /* faces */
+  const double* source;   /* cells */
+  const int* across_j0;   /* cells_i entries, or NULL for none */
+} cfd_cg_system;
+
+/* conjugateGradient (LinearSystem.hpp:315-316, LinearSystem.cpp:118-210) on
+ * the device: x (device, cells) is the starting guess in and the solution
+ * out; report (host, 4 doubles, may be NULL) = {iterations, initial residual,
+ * final residual, converged}; both residuals are L1 norms as in the
+ * reference. Allocates its scratch (two coefficient arrays, five vectors) for
+ * the call. stream: a cudaStream_t, or NULL for the legacy default stream.
+ * Returns after the solve has finished. */
+cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance,
+                        int max_iterations, double* report, void* stream);
+
 /* ---- batches: many solves in one launch ------------------------------------
  * A batch is a descriptor table over existing handles (each keeps its own
  * device state). One launch runs every solve of the table, one thread-block
