@@ -175,6 +175,7 @@ _sig("cfd_mesh_nodes", _P, _P)
 _sig("cfd_mesh_face_conditions", C.c_int, _P, C.c_double, C.c_double, _P, _P, _P)
 _sig("cfd_mesh_free", None, _P)
 _sig("cfd_cg_solve", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
+_sig("cfd_cg_solve_noalloc", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
 _sig("cfd_batch_iterate", C.c_int, _P, C.c_int, C.c_double, _P, _P)
 _sig("cfd_batch_launch", C.c_int, _P, C.c_int, _P)
@@ -434,6 +435,17 @@ def cg_solve(system: CgSystem, x_ptr: int, tolerance: float, max_iterations: int
     report = np.zeros(4)
     _check(_lib.cfd_cg_solve(C.byref(system), C.c_void_p(x_ptr), tolerance, max_iterations,
                              _ptr(report), None if stream is None else C.c_void_p(stream)))
+    return report
+
+
+def cg_solve_noalloc(system: CgSystem, x_ptr: int, tolerance: float, max_iterations: int,
+                     stream: int | None = None) -> np.ndarray:
+    """cfd_cg_solve without allocating: scratch is the library's fixed device
+    array (blocks up to 65,536 nodes; calls must not overlap on the GPU)."""
+    report = np.zeros(4)
+    _check(_lib.cfd_cg_solve_noalloc(C.byref(system), C.c_void_p(x_ptr), tolerance,
+                                     max_iterations, _ptr(report),
+                                     None if stream is None else C.c_void_p(stream)))
     return report
 
 

@@ -14,6 +14,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "cfd_gpu.h"
@@ -256,6 +257,112 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   }
   cudaFree(scratch);
   return st;
+}
+
+}  // extern "C"
+
+// ---- the same solve without allocating ----------------------------------------------
+//
+// Some callers cannot call cudaMalloc: a host application whose memory manager
+// has reserved the whole device up front (a cudaMalloc outside that manager
+// fails or breaks its accounting), or a latency-critical loop that must not
+// block on the implicit device-wide synchronisation cudaFree performs.
+// cfd_cg_solve_noalloc serves them. Its scratch (both coefficient families,
+// the five CG vectors, the wake map and the report) is one file-scope device
+// array of fixed size, so a call allocates nothing; the caller still provides
+// the system and x in its own device memory.
+//
+// Limits and sharing:
+//   * blocks of at most kNoAllocMaxNodes mesh nodes, (cells_i+1)*(cells_j+1)
+//     <= 65,536 (the 384 x 96 medium C-grid has 37,345); larger blocks are
+//     refused with CFD_OUT_OF_RANGE. The array is 3.8 MiB, held by every GPU
+//     that loads this library until the process exits.
+//   * every call shares the one array per device and it keeps the last
+//     call's contents. Nothing in it needs clearing: each word a solve reads is
+//     written earlier in the same call (coefficients and wake map by the layout
+//     launch, r, z and d0 from the start vector, q and d1 before their first
+//     use). Calls whose work overlaps on the GPU (other host threads, or other
+//     streams of this one) race on the array and must be serialised by the
+//     caller.
+//   * the first call on each device resolves the array's device address with
+//     cudaGetSymbolAddress, with that device current; make that first call
+//     before any stream capture.
+
+namespace cfdb {
+namespace {
+
+constexpr long long kNoAllocMaxNodes = 65536;
+// 7 arrays of at most kNoAllocMaxNodes doubles (two face families and five
+// cell vectors, each at most (cells_i+1)*(cells_j+1) long), 4 report words,
+// and the wake map (cells_i ints) in the last kNoAllocMaxNodes/2 doubles.
+constexpr std::size_t kNoAllocDoubles = 7 * kNoAllocMaxNodes + 4 + kNoAllocMaxNodes / 2;
+
+static __device__ __align__(256) double g_noAllocScratch[kNoAllocDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noAllocMutex;
+double* g_noAllocAddress[kMaxDevices] = {};
+
+/// Device address of g_noAllocScratch on the current device, resolved once.
+Status noAllocScratch(double** out) {
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  if (device < 0 || device >= kMaxDevices) return fail(CFD_OUT_OF_RANGE, "device ordinal too large");
+  std::lock_guard<std::mutex> lock(g_noAllocMutex);
+  if (g_noAllocAddress[device] == nullptr) {
+    void* ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_noAllocScratch);
+    if (e != cudaSuccess) {
+      return fail(CFD_INITIALIZATION_FAILURE, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    }
+    g_noAllocAddress[device] = static_cast<double*>(ptr);
+  }
+  *out = g_noAllocAddress[device];
+  return CFD_OK;
+}
+
+}  // namespace
+}  // namespace cfdb
+
+extern "C" {
+
+cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double tolerance,
+                                int max_iterations, double* report, void* stream) {
+  cfdb::CgView V{};
+  if (cfd_status st = cfdb::cgCheck(system, x, max_iterations, &V); st != CFD_OK) return st;
+  const long long nodes = static_cast<long long>(V.NI + 1) * (V.NJ + 1);
+  if (nodes > cfdb::kNoAllocMaxNodes) {
+    return cfdb::fail(CFD_OUT_OF_RANGE,
+                      "cfd_cg_solve_noalloc: block of " + std::to_string(nodes) +
+                          " nodes exceeds the fixed scratch limit of 65536 nodes "
+                          "((cells_i+1)*(cells_j+1)); use cfd_cg_solve");
+  }
+  double* base = nullptr;
+  if (cfd_status st = cfdb::noAllocScratch(&base); st != CFD_OK) return st;
+  const std::size_t slot = static_cast<std::size_t>(cfdb::kNoAllocMaxNodes);
+  V.pN = base + 0 * slot;
+  V.pE = base + 1 * slot;
+  V.r = base + 2 * slot;
+  V.z = base + 3 * slot;
+  V.q = base + 4 * slot;
+  V.d0 = base + 5 * slot;
+  V.d1 = base + 6 * slot;
+  V.report = base + 7 * slot;
+  V.acrossJ0 = reinterpret_cast<const int*>(base + 7 * slot + 4);
+  V.diag = system->diag;
+  V.b = system->source;
+  V.x = x;
+  V.maxIt = max_iterations;
+  V.tol = tolerance;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (cfd_status st = cfdb::cgRun(system, V, s); st != CFD_OK) return st;
+  double host[4];
+  cudaError_t e = cudaMemcpyAsync(host, V.report, sizeof(host), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  if (report != nullptr) for (int k = 0; k < 4; ++k) report[k] = host[k];
+  return CFD_OK;
 }
 
 }  // extern "C"

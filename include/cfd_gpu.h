@@ -218,6 +218,20 @@ typedef struct cfd_cg_system {
 cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance,
                         int max_iterations, double* report, void* stream);
 
+/* The same solve for callers that cannot allocate device memory: a host
+ * application whose memory manager owns the whole device, or a loop that must
+ * not block on cudaFree's device-wide synchronisation. No counterpart in the
+ * reference. It calls no cudaMalloc, cudaFree or allocating library routine:
+ * its scratch is a fixed device array inside this library (3.8 MiB per GPU
+ * that loads it, kept until exit), so blocks are limited to
+ * (cells_i+1)*(cells_j+1) <= 65536 nodes; larger ones return
+ * CFD_OUT_OF_RANGE. All calls on a device share that array; calls that
+ * overlap on the GPU race and must be serialised by the caller. The first call
+ * on each device resolves the array's address; make it before any stream
+ * capture. Results equal cfd_cg_solve's. */
+cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double tolerance,
+                                int max_iterations, double* report, void* stream);
+
 /* ---- batches: many solves in one launch ------------------------------------
  * A batch is a descriptor table over existing handles (each keeps its own
  * device state). One launch runs every solve of the table, one thread-block
