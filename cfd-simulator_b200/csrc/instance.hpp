@@ -50,6 +50,10 @@ enum Stage : int {
   kStageEnd
 };
 
+// Kernel implementation flags (bit mask).
+constexpr int kFlagGlobalCg = 1;
+constexpr int kFlagPlainWavefront = 2;
+
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {
   kMonContinuity = 0, kMonMomX, kMonMomY, kMonMassImbalance, kMonMaxDivergence,

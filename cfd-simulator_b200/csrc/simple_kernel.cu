@@ -38,6 +38,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 
 #include <string>
 
@@ -398,6 +399,150 @@ DEV void gsWavefrontSweeps(const Instance& I, Team& t, int sweeps, const double*
         if (nN >= 0) off += aN[c] * x[nN];
         if (nW >= 0) off += aW[c] * x[nW];
         x[c] = (b[c] - off) / dd;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+/// Block-wide exclusive scan of affine maps x -> p + q x composed in thread
+/// order: each thread passes the composition (p, q) of its own elements
+/// (identity (0, 1) if none) and receives the composition of all elements of
+/// lower threads. Uses sc[0 .. 2*warps) of shared memory; two __syncthreads.
+DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
+  // inclusive scan within the warp (later maps applied after earlier ones)
+  double ip = p, iq = q;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double pp = __shfl_up_sync(0xffffffffu, ip, off);
+    const double qq = __shfl_up_sync(0xffffffffu, iq, off);
+    if (lane >= off) {
+      ip = ip + iq * pp;
+      iq = iq * qq;
+    }
+  }
+  // exclusive within the warp
+  double ep = __shfl_up_sync(0xffffffffu, ip, 1);
+  double eq = __shfl_up_sync(0xffffffffu, iq, 1);
+  if (lane == 0) {
+    ep = 0.0;
+    eq = 1.0;
+  }
+  if (lane == 31) {
+    sc[2 * warp] = ip;
+    sc[2 * warp + 1] = iq;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    double wp = (lane < nwarps) ? sc[2 * lane] : 0.0;
+    double wq = (lane < nwarps) ? sc[2 * lane + 1] : 1.0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double pp = __shfl_up_sync(0xffffffffu, wp, off);
+      const double qq = __shfl_up_sync(0xffffffffu, wq, off);
+      if (lane >= off) {
+        wp = wp + wq * pp;
+        wq = wq * qq;
+      }
+    }
+    double xp = __shfl_up_sync(0xffffffffu, wp, 1);
+    double xq = __shfl_up_sync(0xffffffffu, wq, 1);
+    if (lane == 0) {
+      xp = 0.0;
+      xq = 1.0;
+    }
+    if (lane < nwarps) {
+      sc[2 * lane] = xp;
+      sc[2 * lane + 1] = xq;
+    }
+  }
+  __syncthreads();
+  // earlier warps first, then the earlier lanes of this warp
+  const double wp = sc[2 * warp], wq = sc[2 * warp + 1];
+  p = ep + eq * wp;
+  q = eq * wq;
+}
+
+/// Lexicographic Gauss-Seidel sweeps of one system (LinearSystem.cpp:77-116)
+/// computed row by row. With row j-1 already updated and row j+1 and the
+/// east neighbours still holding their old values, the cell-order update of
+/// row j is the first-order recurrence x_i = p_i + q_i x_{i-1},
+///   p_i = (b_i - aS x_S - aE x_E - aN x_N) / a_P,  q_i = -aW / a_P,
+/// solved by a block-wide scan. Row 0 is split in two: the wake-cut partner
+/// (NI-1-i, 0) of (i, 0) comes later in the row for i < NI/2 (old value) and
+/// earlier for i >= NI/2 (new value), so the second half is solved after the
+/// first. A cell with a_P = 0 keeps its value (p = x, q = 0). This is the
+/// reference's sweep map; only the rounding differs from cell-by-cell order.
+///
+/// Run by every thread of one CTA. Needs NI <= 8 * blockDim.x and
+/// 2 * NI + 2 * warps doubles of shared memory.
+DEV void gsRowScanSweeps(const Instance& I, int sweeps, const double* D, const double* cS,
+                         const double* cN, const double* cW, const double* cE, const double* b,
+                         double* x, double* smem) {
+  const int NI = I.NI, NJ = I.NJ;
+  const int T = blockDim.x;
+  const int per = (NI + T - 1) / T;  // contiguous cells per thread
+  double* rowNew = smem;             // row j, new values
+  double* rowPrev = smem + NI;       // row j - 1, new values
+  double* sc = smem + 2 * NI;
+  const int i0 = threadIdx.x * per;
+  for (int sweep = 0; sweep < sweeps; ++sweep) {
+    for (int j = 0; j < NJ; ++j) {
+      const int segments = (j == 0) ? 2 : 1;
+      double carry = 0.0;
+      for (int seg = 0; seg < segments; ++seg) {
+        const int lo = (segments == 1) ? 0 : (seg == 0 ? 0 : NI / 2);
+        const int hi = (segments == 1) ? NI : (seg == 0 ? NI / 2 : NI);
+        double pv[8], qv[8];
+        double P = 0.0, Q = 1.0;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          pv[e] = 0.0;
+          qv[e] = 1.0;
+          const int i = i0 + e;
+          if (e >= per || i < lo || i >= hi) continue;
+          const int c = j * NI + i;
+          const double d = D[c];
+          if (!(fabs(d) > 0.0)) {
+            pv[e] = x[c];
+            qv[e] = 0.0;
+          } else {
+            double off = 0.0;
+            if (j > 0) {
+              off += cS[c] * rowPrev[i];
+            } else {
+              const int a = I.acrossJ0[i];
+              if (a >= 0) off += cS[c] * ((a < i) ? rowNew[a] : x[a]);
+            }
+            if (i < NI - 1) off += cE[c] * x[c + 1];
+            if (j < NJ - 1) off += cN[c] * x[c + NI];
+            pv[e] = (b[c] - off) / d;
+            qv[e] = (i > 0) ? -cW[c] / d : 0.0;
+          }
+          P = pv[e] + qv[e] * P;
+          Q = qv[e] * Q;
+        }
+        blockAffineExclusiveScan(P, Q, sc);
+        double xv = P + Q * carry;  // value entering this thread's chunk
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int i = i0 + e;
+          if (e >= per || i < lo || i >= hi) continue;
+          xv = pv[e] + qv[e] * xv;
+          rowNew[i] = xv;
+        }
+        __syncthreads();
+        if (hi > lo) carry = rowNew[hi - 1];
+      }
+      // Publish row j: global memory (east/north reads of later rows and the
+      // next sweep) and rowPrev (the south values of row j + 1). Every read
+      // of this row's old values and of rowPrev happened before the scan's
+      // barriers above.
+      for (int i = threadIdx.x; i < NI; i += T) {
+        x[j * NI + i] = rowNew[i];
+        rowPrev[i] = rowNew[i];
       }
       __syncthreads();
     }
@@ -796,6 +941,130 @@ DEV void phaseSstFinish(const Instance& I, Team& t, double (&mx)[8]) {
   }
 }
 
+// ---- pressure CG with the band in shared memory -----------------------------------
+
+/// Shared-memory CG layout: 11 arrays of `stride` doubles per CTA, where
+/// stride = ceil(NJ / R) * NI is the largest band of rows any rank holds, so
+/// every CTA lays its arrays out identically and a neighbour's value is found
+/// at the same offset through DSMEM.
+enum CgSmemArray : int { kSD = 0, kSS, kSN, kSW, kSE, kSX, kSR, kSZ, kSQ, kSD0, kSD1, kCgArrays };
+
+__host__ __device__ inline int cgSmemStride(int NI, int NJ, int R) { return ((NJ + R - 1) / R) * NI; }
+
+/// Where cell n lives during the shared-memory CG: this CTA's band, or the
+/// band just below or just above it (the only other rows a 5-point stencil
+/// reaches; the wake partner of a row-0 cell is in row 0).
+struct Band {
+  int c0, c1, NI, NJ, R, rank;
+  int cBelow, cAbove;  // first cell of the neighbouring bands
+};
+
+DEV int bandFirstCell(int NI, int NJ, int R, int r) { return NI * ((NJ * r) / R); }
+
+/// Jacobi-PCG identical in arithmetic, cell order and reduction order to the
+/// global-memory loop; the vectors and rows of the band stay in shared
+/// memory and the halo rows are read from the neighbouring CTAs. Returns the
+/// iterations run; x is written back to global memory at the end.
+DEV int cgShared(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double rz) {
+  const int stride = cgSmemStride(I.NI, I.NJ, static_cast<int>(t.R));
+  double* a[kCgArrays];
+#pragma unroll
+  for (int k = 0; k < kCgArrays; ++k) a[k] = dyn + k * stride;
+  const int NI = I.NI, NJ = I.NJ;
+  const int R = static_cast<int>(t.R), rank = static_cast<int>(t.rank);
+  const int cBelow = (rank > 0) ? bandFirstCell(NI, NJ, R, rank - 1) : 0;
+  const int cAbove = t.c1;  // the band above starts where this one ends
+  // Remote (DSMEM) views of the neighbouring bands' z, d0 and d1.
+  const double* zB = (rank > 0) ? t.cl.map_shared_rank(a[kSZ], rank - 1) : nullptr;
+  const double* dB0 = (rank > 0) ? t.cl.map_shared_rank(a[kSD0], rank - 1) : nullptr;
+  const double* dB1 = (rank > 0) ? t.cl.map_shared_rank(a[kSD1], rank - 1) : nullptr;
+  const double* zA = (rank < R - 1) ? t.cl.map_shared_rank(a[kSZ], rank + 1) : nullptr;
+  const double* dA0 = (rank < R - 1) ? t.cl.map_shared_rank(a[kSD0], rank + 1) : nullptr;
+  const double* dA1 = (rank < R - 1) ? t.cl.map_shared_rank(a[kSD1], rank + 1) : nullptr;
+
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int k = c - t.c0;
+    const int i = c % NI, j = c / NI;
+    a[kSD][k] = I.pD[c];
+    a[kSS][k] = (j > 0) ? I.pN[j * NI + i] : ((I.acrossJ0[i] >= 0) ? I.pN[i] : 0.0);
+    a[kSN][k] = (j < NJ - 1) ? I.pN[(j + 1) * NI + i] : 0.0;
+    a[kSW][k] = (i > 0) ? I.pE[j * (NI + 1) + i] : 0.0;
+    a[kSE][k] = (i < NI - 1) ? I.pE[j * (NI + 1) + i + 1] : 0.0;
+    a[kSX][k] = 0.0;
+    a[kSR][k] = I.r[c];
+    a[kSZ][k] = I.z[c];
+    a[kSD0][k] = I.d0[c];
+  }
+  t.cl.sync();  // every band loaded before anyone reads a neighbour's
+
+  int cgIters = 0;
+  double beta = 0.0;
+  int cur = 0;  // which d buffer holds the current direction (0: d0, 1: d1)
+  const int op1[1] = {kSum};
+  const int op2[2] = {kSum, kSum};
+  for (int iter = 0; iter < I.cgMax; ++iter) {
+    double* dCur = a[cur ? kSD1 : kSD0];
+    double* dNext = a[cur ? kSD0 : kSD1];
+    const double* dBc = cur ? dB1 : dB0;
+    const double* dAc = cur ? dA1 : dA0;
+    double dAd[1] = {0.0};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int k = c - t.c0;
+      const int i = c % NI, j = c / NI;
+      // value of the direction at cell n: d itself on the first iteration,
+      // z + beta d afterwards; n in this band, or in the band below/above
+      auto dirAt = [&](int n) -> double {
+        if (n >= t.c0 && n < t.c1) {
+          const int m = n - t.c0;
+          return (iter == 0) ? dCur[m] : a[kSZ][m] + beta * dCur[m];
+        }
+        if (n < t.c0) {
+          const int m = n - cBelow;
+          return (iter == 0) ? dBc[m] : zB[m] + beta * dBc[m];
+        }
+        const int m = n - cAbove;
+        return (iter == 0) ? dAc[m] : zA[m] + beta * dAc[m];
+      };
+      const double dc = (iter == 0) ? dCur[k] : a[kSZ][k] + beta * dCur[k];
+      if (iter > 0) dNext[k] = dc;
+      double y = a[kSD][k] * dc;
+      int n = (j > 0) ? c - NI : I.acrossJ0[i];
+      if (n >= 0) y += a[kSS][k] * dirAt(n);
+      if (j < NJ - 1) y += a[kSN][k] * dirAt(c + NI);
+      if (i > 0) y += a[kSW][k] * dirAt(c - 1);
+      if (i < NI - 1) y += a[kSE][k] * dirAt(c + 1);
+      a[kSQ][k] = y;
+      dAd[0] += dc * y;
+    }
+    if (iter > 0) cur ^= 1;
+    teamReduce(t, sh, dAd, op1);
+    if (!(fabs(dAd[0]) > 0.0)) break;
+    const double step = rz / dAd[0];
+    double* dNow = a[cur ? kSD1 : kSD0];
+    double rr[2] = {0.0, 0.0};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int k = c - t.c0;
+      a[kSX][k] += step * dNow[k];
+      const double rc = a[kSR][k] - step * a[kSQ][k];
+      a[kSR][k] = rc;
+      const double dg = a[kSD][k];
+      const double zc = (fabs(dg) > 0.0) ? rc / dg : rc;
+      a[kSZ][k] = zc;
+      rr[0] += fabs(rc);
+      rr[1] += rc * zc;
+    }
+    teamReduce(t, sh, rr, op2);
+    cgIters = iter + 1;
+    if (rr[0] <= I.cgTol * initial) break;
+    if (!(fabs(rz) > 0.0)) break;
+    beta = rr[1] / rz;
+    rz = rr[1];
+  }
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] = a[kSX][c - t.c0];
+  t.cl.sync();  // x visible to the correction; no peer still reads this band
+  return cgIters;
+}
+
 }  // namespace
 
 // ---- the kernel -----------------------------------------------------------------
@@ -804,17 +1073,25 @@ DEV void phaseSstFinish(const Instance& I, Team& t, double (&mx)[8]) {
 /// iteration early; `tolerance` >= 0 stops at convergence or divergence as
 /// SolverWorker does, SolverWorker.cpp:164-185). One cluster per instance.
 __global__ void __launch_bounds__(512, 1)
-simpleKernel(const Instance* __restrict__ instances, int iterations, int stopStage, double tolerance) {
+simpleKernel(const Instance* __restrict__ instances, int iterations, int stopStage, double tolerance,
+             int smemBytes, int flags) {
   __shared__ Shared sh;
+  extern __shared__ double dyn[];
   Team t{cg::this_cluster(), 0, 0, 0, 0, 0, 0, 0};
   t.rank = t.cl.block_rank();
   t.R = t.cl.num_blocks();
   t.tid = threadIdx.x;
   t.T = blockDim.x;
   const Instance& I = instances[blockIdx.x / t.R];
-  t.c0 = static_cast<int>((static_cast<long long>(I.N) * t.rank) / t.R);
-  t.c1 = static_cast<int>((static_cast<long long>(I.N) * (t.rank + 1)) / t.R);
+  // Each CTA owns a band of whole rows; the same split in every phase.
+  t.c0 = I.NI * ((I.NJ * static_cast<int>(t.rank)) / static_cast<int>(t.R));
+  t.c1 = I.NI * ((I.NJ * (static_cast<int>(t.rank) + 1)) / static_cast<int>(t.R));
   const bool sst = (I.model == 2);
+  // The pressure CG keeps its band in shared memory when every band has a
+  // row and the largest band's 11 arrays fit in what the launch provides.
+  const bool cgInShared =
+      !(flags & kFlagGlobalCg) && I.NJ >= static_cast<int>(t.R) &&
+      static_cast<long long>(kCgArrays) * cgSmemStride(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
   const bool leader = (t.rank == 0 && t.tid == 0);
 
   int done = 0;
@@ -898,7 +1175,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       const double initial = init[0];
       double rz = init[1];
       int cgIters = 0;
-      if (initial > 0.0) {
+      if (initial > 0.0 && cgInShared) {
+        cgIters = cgShared(I, t, sh, dyn, initial, rz);
+      } else if (initial > 0.0) {
         double* dCur = I.d0;
         double* dNext = I.d1;
         double beta = 0.0;
@@ -994,8 +1273,21 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       // k and omega sweep in the reference's cell order: their floors and
       // the wall-cell omega override act after the sweeps, so the converged
       // state depends on the order (a colouring would move it by ~1e-3).
-      gsWavefrontSweeps(I, t, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN, I.wW,
-                        I.wE, I.wB, I.om);
+      if (!(flags & kFlagPlainWavefront) && I.NI <= 8 * t.T &&
+          (2 * I.NI + 64) * 8 <= smemBytes) {
+        // rank 0 sweeps k, rank 1 omega (one CTA: both, one after the other)
+        if (t.R == 1) {
+          gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
+          gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
+        } else if (t.rank == 0) {
+          gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
+        } else if (t.rank == 1) {
+          gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
+        }
+      } else {
+        gsWavefrontSweeps(I, t, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN,
+                          I.wW, I.wE, I.wB, I.om);
+      }
       t.cl.sync();
       if (stopStage == kStageSstSolve) { done = it + 1; break; }
 
@@ -1073,18 +1365,43 @@ int chooseClusterSize(int cells) {
   return r;
 }
 
+int kernelFlags() {
+  // Implementation choices for tuning comparisons (results are identical):
+  // bit 0 keeps the pressure CG in global memory, bit 1 uses the plain
+  // wavefront sweeps.
+  static const int flags = [] {
+    const char* env = std::getenv("CFD_KERNEL_FLAGS");
+    return (env != nullptr) ? std::atoi(env) : 0;
+  }();
+  return flags;
+}
+
+int cgSharedBytes(int NI, int NJ, int clusterSize) {
+  // The k/omega row sweeps keep two rows and the scan's warp totals.
+  const long long wave = (2LL * NI + 64) * 8;
+  long long bytes = 0;
+  if (NJ >= clusterSize) bytes = static_cast<long long>(kCgArrays) * cgSmemStride(NI, NJ, clusterSize) * 8;
+  if (bytes > kMaxCgSharedBytes) bytes = 0;
+  if (bytes < wave && wave <= kMaxCgSharedBytes) bytes = wave;
+  return static_cast<int>(bytes);
+}
+
 Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
-                    int iterations, int stopStage, double tolerance, cudaStream_t stream) {
+                    int iterations, int stopStage, double tolerance, cudaStream_t stream,
+                    int smemBytes) {
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) {
+      e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxCgSharedBytes);
+    }
     if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
     configured = true;
   }
   cudaLaunchConfig_t config = {};
   config.gridDim = dim3(static_cast<unsigned>(count * clusterSize), 1, 1);
   config.blockDim = dim3(static_cast<unsigned>(threads), 1, 1);
-  config.dynamicSmemBytes = 0;
+  config.dynamicSmemBytes = static_cast<size_t>(smemBytes);
   config.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1093,7 +1410,8 @@ Status launchSimple(const Instance* dInstances, int count, int clusterSize, int 
   attr[0].val.clusterDim.z = 1;
   config.attrs = attr;
   config.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&config, simpleKernel, dInstances, iterations, stopStage, tolerance);
+  cudaError_t e = cudaLaunchKernelEx(&config, simpleKernel, dInstances, iterations, stopStage, tolerance,
+                                     smemBytes, kernelFlags());
   if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, std::string("SIMPLE kernel launch: ") + cudaGetErrorString(e));
   return CFD_OK;
 }

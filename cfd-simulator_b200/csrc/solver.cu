@@ -226,6 +226,11 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
   for (int i = 0; i < NI_; ++i) {
     const int a = (neighbour_[i] < 0) ? across_[i] : -1;
     acrossJ0[i] = a;
+    if (a >= NI_) return fail(CFD_NOT_IMPLEMENTED, "a wake-cut partner must lie in the j = 0 row");
+    // The C-grid pairing (CGrid.cpp:368-378): column i meets column NI-1-i.
+    if (a >= 0 && a != NI_ - 1 - i) {
+      return fail(CFD_NOT_IMPLEMENTED, "wake-cut partners must pair column i with column cellsI-1-i");
+    }
     if (a >= 0) {
       const int ai = a % NI_, aj = a / NI_;
       if (((ai + aj) & 1) == (i & 1)) {
@@ -613,7 +618,8 @@ Status Solver::iterate(int n, int stopStage, double tolerance, std::vector<doubl
   int total = 0;
   while (total < n) {
     const int chunk = std::min(n - total, historyCapacity_);
-    if (Status st = launchSimple(dView_, 1, clusterSize_, threads_, chunk, stopStage, tolerance, stream_);
+    if (Status st = launchSimple(dView_, 1, clusterSize_, threads_, chunk, stopStage, tolerance, stream_,
+                                 cgSharedBytes(NI_, NJ_, clusterSize_));
         st != CFD_OK) {
       return st;
     }
@@ -921,6 +927,7 @@ struct cfd_batch_t {
   cudaStream_t stream{nullptr};
   int clusterSize{1};
   int threads{512};
+  int smemBytes{0};
   int lastIterations{0};
 };
 
@@ -954,6 +961,10 @@ cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out
     b->clusterSize = std::max(b->clusterSize, solvers[k]->solver->clusterSize());
     b->threads = solvers[k]->solver->threads();
   }
+  for (cfd_handle h : b->handles) {
+    b->smemBytes = std::max(b->smemBytes, cfdb::cgSharedBytes(h->solver->cellsI(), h->solver->cellsJ(),
+                                                              b->clusterSize));
+  }
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dTable), count * sizeof(cfdb::Instance));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -974,7 +985,7 @@ cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream) {
   cudaStream_t s = (stream != nullptr) ? static_cast<cudaStream_t>(stream) : b->stream;
   b->lastIterations = n;
   return cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize, b->threads, n,
-                            cfdb::kStageEnd, -1.0, s);
+                            cfdb::kStageEnd, -1.0, s, b->smemBytes);
 }
 
 cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last) {
@@ -1010,7 +1021,8 @@ cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_mon
       if (!h->solver->initialised()) return cfdb::fail(CFD_INVALID_ARGUMENT, "a solver in the batch is not initialised");
     }
     if (cfd_status st = cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize,
-                                           b->threads, chunk, cfdb::kStageEnd, tol, b->stream);
+                                           b->threads, chunk, cfdb::kStageEnd, tol, b->stream,
+                                           b->smemBytes);
         st != CFD_OK) {
       return st;
     }

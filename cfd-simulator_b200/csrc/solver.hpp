@@ -140,7 +140,13 @@ Status launchWallDistance(int n, const double* centroid, int walls, const double
                           double far, double* out, cudaStream_t stream);
 
 Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
-                    int iterations, int stopStage, double tolerance, cudaStream_t stream);
+                    int iterations, int stopStage, double tolerance, cudaStream_t stream,
+                    int smemBytes);
+
+/// Dynamic shared memory the pressure CG needs to keep a solve's band on
+/// chip (0: it does not fit and the CG runs from global memory).
+int cgSharedBytes(int NI, int NJ, int clusterSize);
+constexpr int kMaxCgSharedBytes = 210 * 1024;
 
 /// Cluster size used for a solve of `cells` cells (power of two, 1..16).
 int chooseClusterSize(int cells);
