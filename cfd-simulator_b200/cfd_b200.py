@@ -77,7 +77,8 @@ class MeshDesc(C.Structure):
                 ("cell_areas", C.c_void_p), ("face_centres", C.c_void_p),
                 ("face_normals", C.c_void_p), ("face_areas", C.c_void_p),
                 ("face_owner", C.c_void_p), ("face_neighbour", C.c_void_p),
-                ("face_boundary", C.c_void_p), ("face_partner", C.c_void_p)]
+                ("face_boundary", C.c_void_p), ("face_partner", C.c_void_p),
+                ("nodes", C.c_void_p)]
 
 
 class FaceBc(C.Structure):
@@ -135,6 +136,15 @@ class Monitor(C.Structure):
         return max(abs(self.continuity), abs(self.momentum_x), abs(self.momentum_y))
 
 
+class Forces(C.Structure):
+    _fields_ = [("lift_coefficient", C.c_double), ("drag_coefficient", C.c_double),
+                ("moment_coefficient", C.c_double), ("pressure_drag_coefficient", C.c_double),
+                ("friction_drag_coefficient", C.c_double), ("lift", C.c_double),
+                ("drag", C.c_double), ("pitching_moment", C.c_double),
+                ("stagnation_chord_fraction", C.c_double), ("stations", C.c_int),
+                ("leading_edge", C.c_int)]
+
+
 class CGridOptions(C.Structure):
     _fields_ = [("upstream_chords", C.c_double), ("downstream_chords", C.c_double),
                 ("vertical_chords", C.c_double), ("surface_points", C.c_int),
@@ -163,6 +173,8 @@ _sig("cfd_gpu_iterate_partial", C.c_int, _P, C.c_int, _P)
 _sig("cfd_gpu_read_field", C.c_int, _P, C.c_int, _P)
 _sig("cfd_gpu_load_state", C.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P)
 _sig("cfd_gpu_set_settings", C.c_int, _P, _P)
+_sig("cfd_gpu_forces", C.c_int, _P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+     _P, _P, _P)
 _sig("cfd_gpu_dims", C.c_int, _P, _P)
 _sig("cfd_gpu_scalars", C.c_int, _P, _P)
 _sig("cfd_gpu_destroy", C.c_int, _P)
@@ -239,6 +251,7 @@ class MeshArrays:
                           ("face_neighbour", self.neighbour), ("face_boundary", self.boundary),
                           ("face_partner", self.partner)):
             setattr(d, name, arr.ctypes.data)
+        d.nodes = None if self.nodes is None else self.nodes.ctypes.data
         return d
 
 
@@ -404,6 +417,18 @@ class SimpleSolver:
 
     def set_settings(self, settings: Settings) -> None:
         _check(_lib.cfd_gpu_set_settings(self._h, C.byref(settings)))
+
+    def forces(self, speed: float, alpha_deg: float, density: float = 1.0,
+               reference_pressure: float = 0.0, chord: float = 1.0):
+        """extractSurface + integrateForces on the device: (Forces, Cp, Cf),
+        stations upper (leading edge onwards) then lower."""
+        f = Forces()
+        cap = self.mesh.cells_i
+        cp = np.zeros(cap)
+        cf = np.zeros(cap)
+        _check(_lib.cfd_gpu_forces(self._h, speed, alpha_deg, density, reference_pressure, chord,
+                                   C.byref(f), _ptr(cp), _ptr(cf)))
+        return f, cp[: f.stations], cf[: f.stations]
 
     def scalars(self) -> np.ndarray:
         out = np.zeros(3)

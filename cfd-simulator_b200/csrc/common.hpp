@@ -43,6 +43,7 @@ inline void describe(const HostMesh& g, cfd_mesh_desc* d) {
   d->face_neighbour = g.neighbour.data();
   d->face_boundary = g.boundary.data();
   d->face_partner = g.partner.data();
+  d->nodes = g.nodes.data();
 }
 
 }  // namespace cfdb

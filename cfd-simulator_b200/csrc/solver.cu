@@ -263,6 +263,24 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     wallMask[o] |= static_cast<uint8_t>(1u << bit);
   }
 
+  // Wall stations for the device force integration (needs node coordinates).
+  {
+    HostMesh view;
+    view.nodesI = ni;
+    view.nodesJ = nj;
+    view.cells = N_;
+    view.faces = F_;
+    view.centroid = centroid_;
+    view.faceCentre = faceCentre_;
+    view.faceNormal = faceNormal_;
+    view.owner = owner_;
+    view.neighbour = neighbour_;
+    view.boundary = boundary_;
+    view.partner = partner_;
+    if (Status st = buildWallTable(view, m.nodes, &wall_); st != CFD_OK) return st;
+  }
+  const std::size_t S = static_cast<std::size_t>(std::max(wall_.count(), 1));
+
   // ---- device layout ----
   const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
   const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
@@ -298,6 +316,16 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     dCentroids_ = a.take<double>(2 * N);
     dWallCentres_ = a.take<double>(std::max<std::size_t>(wallCentres.size(), 2));
     dView_ = a.take<Instance>(1);
+    dWall_.owner = a.take<int>(S);
+    dWall_.second = a.take<int>(S);
+    dWall_.cx = a.take<double>(S); dWall_.cy = a.take<double>(S);
+    dWall_.tx = a.take<double>(S); dWall_.ty = a.take<double>(S);
+    dWall_.nx = a.take<double>(S); dWall_.ny = a.take<double>(S);
+    dWall_.length = a.take<double>(S);
+    dWall_.wallDistance = a.take<double>(S);
+    dWall_.outerDistance = a.take<double>(S);
+    dStations_ = a.take<double>(S * kStationValues);
+    dForces_ = a.take<double>(16);
   };
   carve(arena_);
   if (Status st = arena_.allocate(); st != CFD_OK) return st;
@@ -343,6 +371,21 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
   CUDA_OR_FAIL(cudaMemcpy(dCentroids_, centroid_.data(), 2 * N * sizeof(double), cudaMemcpyHostToDevice));
   if (!wallCentres.empty()) {
     CUDA_OR_FAIL(cudaMemcpy(dWallCentres_, wallCentres.data(), wallCentres.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  dWall_.count = wall_.count();
+  dWall_.leadingEdge = wall_.leadingEdge;
+  if (wall_.count() > 0) {
+    const std::size_t n = wall_.owner.size();
+    CUDA_OR_FAIL(cudaMemcpy(const_cast<int*>(dWall_.owner), wall_.owner.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_OR_FAIL(cudaMemcpy(const_cast<int*>(dWall_.second), wall_.second.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    const std::pair<const double*, const std::vector<double>*> cols[] = {
+        {dWall_.cx, &wall_.cx}, {dWall_.cy, &wall_.cy}, {dWall_.tx, &wall_.tx}, {dWall_.ty, &wall_.ty},
+        {dWall_.nx, &wall_.nx}, {dWall_.ny, &wall_.ny}, {dWall_.length, &wall_.length},
+        {dWall_.wallDistance, &wall_.wallDistance}, {dWall_.outerDistance, &wall_.outerDistance}};
+    for (const auto& col : cols) {
+      CUDA_OR_FAIL(cudaMemcpy(const_cast<double*>(col.first), col.second->data(), n * sizeof(double),
+                              cudaMemcpyHostToDevice));
+    }
   }
   // momentumDiagonal_ starts at 1 (SimpleSolver.cpp:64).
   {
@@ -744,6 +787,51 @@ Status Solver::readField(int which, double* out) {
   return fail(CFD_OUT_OF_RANGE, "unknown field " + std::to_string(which));
 }
 
+Status Solver::forces(double speed, double alphaDeg, double density, double referencePressure,
+                      double chord, double* out, double* cp, double* cf, int* stations,
+                      int* leadingEdge) {
+  if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
+  if (wall_.count() < 4) {
+    return fail(CFD_NOT_FOUND, "no aerofoil surface: the mesh has no wall stations (or no node coordinates)");
+  }
+  if (!std::isfinite(speed) || speed <= 0.0 || !std::isfinite(density) || density <= 0.0) {
+    return fail(CFD_INVALID_ARGUMENT, "freestream speed and density must be positive");
+  }
+  // FreestreamConditions::dynamicPressure and angleOfAttackRad (Freestream.cpp:7-18);
+  // the wind-axis rotation uses the host's cos and sin, as the reference does.
+  const double dynamicPressure = 0.5 * density * speed * speed;
+  const double alpha = alphaDeg * 3.14159265358979323846 / 180.0;
+  const double c = (chord > 0.0) ? chord : 1.0;
+  const Instance& I = view_;
+  if (Status st = launchForces(dWall_, I.p, I.u, I.v, I.mu, dynamicPressure, referencePressure, c,
+                               std::cos(alpha), std::sin(alpha), dStations_, dForces_, stream_);
+      st != CFD_OK) {
+    return st;
+  }
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+  double h[10];
+  CUDA_OR_FAIL(cudaMemcpy(h, dForces_, sizeof(h), cudaMemcpyDeviceToHost));
+  std::copy(h, h + 10, out);
+  const int S = wall_.count();
+  if (stations != nullptr) *stations = S;
+  if (leadingEdge != nullptr) *leadingEdge = wall_.leadingEdge;
+  if (cp != nullptr || cf != nullptr) {
+    std::vector<double> st(static_cast<std::size_t>(S) * kStationValues);
+    CUDA_OR_FAIL(cudaMemcpy(st.data(), dStations_, st.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    // upper: leading edge onwards; lower: from the leading edge back to 0
+    int q = 0;
+    for (int k = wall_.leadingEdge; k < S; ++k, ++q) {
+      if (cp) cp[q] = st[static_cast<std::size_t>(k) * kStationValues + 1];
+      if (cf) cf[q] = st[static_cast<std::size_t>(k) * kStationValues + 3];
+    }
+    for (int k = wall_.leadingEdge - 1; k >= 0; --k, ++q) {
+      if (cp) cp[q] = st[static_cast<std::size_t>(k) * kStationValues + 1];
+      if (cf) cf[q] = st[static_cast<std::size_t>(k) * kStationValues + 3];
+    }
+  }
+  return CFD_OK;
+}
+
 Status Solver::loadState(const double* u, const double* v, const double* p, const double* massFlux,
                          const double* k, const double* omega, const double* mut, const double* muEff) {
   if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
@@ -885,6 +973,33 @@ cfd_status cfd_gpu_load_state(cfd_handle h, const double* u, const double* v, co
                               const double* mut, const double* mu_eff) {
   if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
   return h->solver->loadState(u, v, p, mass_flux, k, omega, mut, mu_eff);
+}
+
+cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double density,
+                          double reference_pressure, double chord, cfd_forces* out, double* cp,
+                          double* cf) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  if (out == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null output");
+  double v[10];
+  int stations = 0, leadingEdge = 0;
+  if (cfd_status st = h->solver->forces(speed, alpha_deg, density, reference_pressure, chord, v, cp, cf,
+                                        &stations, &leadingEdge);
+      st != CFD_OK) {
+    return st;
+  }
+  out->lift_coefficient = v[0];
+  out->drag_coefficient = v[1];
+  out->moment_coefficient = v[2];
+  out->pressure_drag_coefficient = v[3];
+  out->friction_drag_coefficient = v[4];
+  out->lift = v[5];
+  out->drag = v[6];
+  out->pitching_moment = v[7];
+  out->stagnation_chord_fraction = v[8];
+  out->stations = static_cast<int>(v[9]);
+  out->leading_edge = leadingEdge;
+  (void)stations;
+  return CFD_OK;
 }
 
 cfd_status cfd_gpu_set_settings(cfd_handle h, const cfd_settings* settings) {

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "forces.hpp"
 #include "instance.hpp"
 
 namespace cfdb {
@@ -78,6 +79,11 @@ class Solver {
   Status loadState(const double* u, const double* v, const double* p, const double* massFlux,
                    const double* k, const double* omega, const double* mut, const double* muEff);
   Status setSettings(const Settings& s);
+  /// Surface data and forces of the current field (device, FP64). out gets
+  /// the 10 values of launchForces; cp/cf (may be null) one per station in
+  /// upper-then-lower order.
+  Status forces(double speed, double alphaDeg, double density, double referencePressure,
+                double chord, double* out, double* cp, double* cf, int* stations, int* leadingEdge);
 
   int cellsI() const { return NI_; }
   int cellsJ() const { return NJ_; }
@@ -120,6 +126,11 @@ class Solver {
   std::vector<int> across_;                          // oppositeCell per face
   std::vector<double> muMol_;
   std::vector<double> wallDist_;
+
+  HostWallTable wall_;
+  WallTable dWall_{};
+  double* dStations_{nullptr};
+  double* dForces_{nullptr};
 
   DeviceArena arena_;
   Instance view_{};

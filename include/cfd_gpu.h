@@ -61,6 +61,8 @@ typedef struct cfd_mesh_desc {
   const int* face_neighbour;     /* faces, -1 on a boundary */
   const int* face_boundary;      /* faces, CFD_FACE_* */
   const int* face_partner;       /* faces, wake-cut partner face or -1 */
+  const double* nodes;           /* 2 * nodes_i * nodes_j, row-major (j, i); may be NULL
+                                    (then cfd_gpu_forces is unavailable) */
 } cfd_mesh_desc;
 
 /* flow::FaceCondition per face (BoundaryConditions.hpp:101-107). */
@@ -166,6 +168,26 @@ cfd_status cfd_gpu_iterate_partial(cfd_handle h, int stage, cfd_monitor* last);
 /* SimpleSolver::field()/massFlux()/divergence() and friends: copy one device
  * field to host memory in reference order (see CFD_FIELD_*). */
 cfd_status cfd_gpu_read_field(cfd_handle h, int which, double* out);
+
+/* Surface data and forces (post::extractSurface + post::integrateForces,
+ * src/post/SurfaceData.cpp:101-348, src/post/Forces.cpp:23-130), computed on
+ * the device in FP64 from the current field: wall Cp, the two-point wall
+ * shear, and the force and quarter-chord moment coefficients in wind axes. */
+typedef struct cfd_forces {
+  double lift_coefficient, drag_coefficient, moment_coefficient;
+  double pressure_drag_coefficient, friction_drag_coefficient;
+  double lift, drag, pitching_moment;
+  double stagnation_chord_fraction;
+  int stations;     /* wall stations: upper (leading edge -> trailing edge) then lower */
+  int leading_edge; /* number of lower-surface stations */
+} cfd_forces;
+
+/* speed, alpha_deg, density and reference_pressure describe the freestream
+ * (FreestreamConditions); chord the section. cp and cf (may be NULL) receive
+ * one value per station in the order of `stations`. Needs mesh nodes. */
+cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double density,
+                          double reference_pressure, double chord, cfd_forces* out, double* cp,
+                          double* cf);
 
 /* Overwrite the solver state (a warm start, or a state to continue from):
  * u, v, p per cell; mass_flux per face (may be NULL to keep); k, omega, mut

@@ -109,3 +109,40 @@ def test_divergence_and_mass_flux_accessors():
     o.iterate(3)
     assert rel_err(d.divergence(), o.read(6)) < 1e-7
     assert d.mass_flux().shape == (c.mesh.faces,)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_forces_on_the_reference_field_match_the_reference(name):
+    """extractSurface + integrateForces on the device, fed the reference's own
+    converged field: Cl, Cd, Cm and every station's Cp as the reference's."""
+    c = Case(name)
+    g = c.g
+    d = c.device()
+    d.load_state(u=g["converged/u"], v=g["converged/v"], p=g["converged/p"],
+                 mu_eff=g["converged/mu_eff"])
+    f, cp, cf = d.forces(1.0, c.alpha, 1.0)
+    ref = g["converged/forces"]
+    for got, want in ((f.lift_coefficient, ref[0]), (f.drag_coefficient, ref[1]),
+                      (f.moment_coefficient, ref[2]), (f.pressure_drag_coefficient, ref[3]),
+                      (f.friction_drag_coefficient, ref[4])):
+        assert got == pytest.approx(want, rel=1e-13, abs=1e-15)
+    assert f.stations == int(ref[5])
+    assert np.max(np.abs(cp - g["converged/cp"])) <= 1e-13 * max(1.0, np.max(np.abs(cp)))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_converged_forces_match_the_reference(name):
+    """Cl, Cd and Cm of a converged device solve within 1e-7 relative of the
+    reference's, and Cp at every station."""
+    c = Case(name)
+    g = c.g
+    d = c.device()
+    tol = 1e-12 if c.model == 0 else 1e-11
+    d.converge(20000, tol)
+    d.iterate(2000)
+    f, cp, _ = d.forces(1.0, c.alpha, 1.0)
+    ref = g["converged/forces"]
+    assert f.lift_coefficient == pytest.approx(ref[0], rel=1e-7)
+    assert f.drag_coefficient == pytest.approx(ref[1], rel=1e-7)
+    assert f.moment_coefficient == pytest.approx(ref[2], rel=1e-7)
+    assert np.max(np.abs(cp - g["converged/cp"])) < 1e-7
