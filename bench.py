@@ -372,6 +372,118 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ------------------------------------------------- engine workloads ---
+
+GRIDS = {  # (surface, wake, normal) points; cells 192x48, 384x96, 768x192
+    "coarse": (64, 33, 49), "medium": (128, 65, 97), "fine": (256, 129, 193),
+}
+
+
+def _percentiles(values):
+    if not values:
+        return {"p50": None, "p95": None, "p99": None}
+    a = np.sort(np.asarray(values))
+    return {f"p{q}": float(np.percentile(a, q)) for q in (50, 95, 99)}
+
+
+def _summarise(results, wall_s, cb):
+    statuses = {}
+    for r in results:
+        statuses[cb.STATUS_NAMES[r.status]] = statuses.get(cb.STATUS_NAMES[r.status], 0) + 1
+    cell_iters = float(sum(r.cells * r.iterations for r in results))
+    lat = [r.finished_s - r.submitted_s for r in results]
+    return {"solves": len(results), "wall_s": wall_s, "solves_per_min": 60.0 * len(results) / wall_s,
+            "cell_iters_per_s": cell_iters / wall_s, "statuses": statuses,
+            "time_to_convergence_s": _percentiles(lat),
+            "iterations": _percentiles([r.iterations for r in results])}
+
+
+def run_polar(args) -> None:
+    """21-point NACA 2412 SST Re 3e6 polar (alpha -4..16 step 1) on
+    the fine 768x192 C-grid, plus NACA 0012 SST Re 1e6 alpha 4 on the coarse,
+    medium and fine grids, all resident at once in one engine."""
+    import torch
+    torch.cuda.set_device(0)
+    import cfd_b200 as cb
+    cb.set_device(0)
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO)
+    reqs = []
+    for alpha in range(-4, 17):
+        s, w, n = GRIDS["fine"]
+        reqs.append(cb.request("2412", float(alpha), 3e6, tolerance=args.tolerance,
+                               max_iterations=args.cap, surface_points=s, wake_points=w,
+                               normal_points=n, first_layer_height=5e-6, settings=settings))
+    for level, fl in (("coarse", 2e-3), ("medium", 1e-5), ("fine", 5e-6)):
+        s, w, n = GRIDS[level]
+        reqs.append(cb.request("0012", 4.0, 1e6, tolerance=args.tolerance, max_iterations=args.cap,
+                               surface_points=s, wake_points=w, normal_points=n,
+                               first_layer_height=fl, settings=settings))
+    engine = cb.Engine(chunk=args.chunk)
+    t0 = time.perf_counter()
+    results = engine.run(reqs)
+    wall = time.perf_counter() - t0
+    out = _summarise(results, wall, cb)
+    out.update({"workload": "polar: NACA2412 SST Re3e6 768x192 alpha -4..16 + NACA0012 SST Re1e6 "
+                            "alpha 4 on 192x48/384x96/768x192", "tolerance": args.tolerance,
+                "cap": args.cap, "chunk": args.chunk,
+                "polar": [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
+                           "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
+                           "iterations": r.iterations, "cl": r.lift_coefficient,
+                           "cd": r.drag_coefficient, "cm": r.moment_coefficient,
+                           "continuity": r.continuity} for r in results]})
+    print(json.dumps(out), flush=True)
+
+
+def serving_stream(n: int, rate: float, seed: int):
+    """seeded Poisson arrivals of NACA 4-digit SST requests."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    out = []
+    for k in range(n):
+        m = int(rng.integers(0, 7))
+        pos = int(rng.integers(2, 7)) if m > 0 else 0
+        thick = int(rng.integers(6, 22))
+        alpha = float(rng.uniform(-5.0, 15.0))
+        re = float(10 ** rng.uniform(5.0, 7.0))
+        level = rng.choice(["coarse", "medium", "fine"], p=[0.5, 0.35, 0.15])
+        out.append((float(t[k]), f"{m}{pos}{thick:02d}", alpha, re, str(level),
+                    2.5e-5 * (1e6 / re) ** 0.9))
+    return out
+
+
+def run_serve(args) -> None:
+    import torch
+    torch.cuda.set_device(0)
+    import cfd_b200 as cb
+    cb.set_device(0)
+    stream = serving_stream(args.requests, args.rate, args.seed)
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO)
+    engine = cb.Engine(chunk=args.chunk)
+    t0 = engine.clock()
+    submitted, results = 0, []
+    wall0 = time.perf_counter()
+    while len(results) < len(stream):
+        now = engine.clock() - t0
+        while submitted < len(stream) and stream[submitted][0] <= now:
+            _, des, alpha, re, level, fl = stream[submitted]
+            s, w, n = GRIDS[level]
+            engine.submit(cb.request(des, alpha, re, tolerance=args.tolerance,
+                                     max_iterations=args.cap, surface_points=s, wake_points=w,
+                                     normal_points=n, first_layer_height=fl, settings=settings))
+            submitted += 1
+        active, queued = engine.step()
+        results.extend(engine.results())
+        if active == 0 and queued == 0 and submitted < len(stream):
+            time.sleep(max(0.0, min(0.05, stream[submitted][0] - (engine.clock() - t0))))
+    wall = time.perf_counter() - wall0
+    out = _summarise(results, wall, cb)
+    out.update({"workload": f"serve: Poisson lambda={args.rate}/s, {args.requests} NACA 4-digit SST "
+                            f"requests (seed {args.seed}), meshes 192x48/384x96/768x192 at "
+                            "0.5/0.35/0.15", "tolerance": args.tolerance, "cap": args.cap,
+                "chunk": args.chunk})
+    print(json.dumps(out), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -379,10 +491,22 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("c2", "polar", "serve"), default="c2",
+                    help="c2: the benchmark line (default); polar / serve: engine workloads")
+    ap.add_argument("--tolerance", type=float, default=1e-6)
+    ap.add_argument("--cap", type=int, default=4000)
+    ap.add_argument("--chunk", type=int, default=32)
+    ap.add_argument("--requests", type=int, default=512)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=20261203)
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
-    if args.impl == "reference":
+    if args.workload == "polar":
+        run_polar(args)
+    elif args.workload == "serve":
+        run_serve(args)
+    elif args.impl == "reference":
         run_reference_arm(args)
     else:
         run_ours(args)

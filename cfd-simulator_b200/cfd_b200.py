@@ -188,6 +188,12 @@ _sig("cfd_mesh_face_conditions", C.c_int, _P, C.c_double, C.c_double, _P, _P, _P
 _sig("cfd_mesh_free", None, _P)
 _sig("cfd_cg_solve", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
 _sig("cfd_cg_solve_noalloc", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
+_sig("cfd_engine_create", C.c_int, C.c_ulonglong, C.c_int, _P)
+_sig("cfd_engine_submit", C.c_int, _P, _P, _P)
+_sig("cfd_engine_step", C.c_int, _P, _P, _P)
+_sig("cfd_engine_results", C.c_int, _P, _P, C.c_int, _P)
+_sig("cfd_engine_clock", C.c_double, _P)
+_sig("cfd_engine_destroy", C.c_int, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
 _sig("cfd_batch_iterate", C.c_int, _P, C.c_int, C.c_double, _P, _P)
 _sig("cfd_batch_launch", C.c_int, _P, C.c_int, _P)
@@ -521,6 +527,102 @@ class Batch:
         cluster, threads = C.c_int(), C.c_int()
         _check(_lib.cfd_batch_shape(self._h, C.byref(cluster), C.byref(threads)))
         return cluster.value, threads.value
+
+
+class Request(C.Structure):
+    _fields_ = [("designation", C.c_char * 8), ("grid_surface_points", C.c_int),
+                ("grid_wake_points", C.c_int), ("grid_normal_points", C.c_int),
+                ("grid_first_layer_height", C.c_double), ("grid_upstream_chords", C.c_double),
+                ("grid_downstream_chords", C.c_double), ("grid_vertical_chords", C.c_double),
+                ("alpha_deg", C.c_double), ("reynolds", C.c_double), ("speed", C.c_double),
+                ("density", C.c_double), ("model", C.c_int), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int), ("settings", Settings)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int), ("status", C.c_int), ("iterations", C.c_int),
+                ("retried_cold", C.c_int), ("cells", C.c_int), ("pad_", C.c_int),
+                ("continuity", C.c_double), ("momentum_x", C.c_double),
+                ("momentum_y", C.c_double), ("lift_coefficient", C.c_double),
+                ("drag_coefficient", C.c_double), ("moment_coefficient", C.c_double),
+                ("pressure_drag_coefficient", C.c_double),
+                ("friction_drag_coefficient", C.c_double), ("submitted_s", C.c_double),
+                ("started_s", C.c_double), ("finished_s", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad_"}
+
+
+STATUS_NAMES = {0: "converged", 1: "iteration-limit", 2: "diverged"}
+
+
+def request(designation: str, alpha_deg: float, reynolds: float, model: int = MODEL_SST,
+            tolerance: float = 1e-6, max_iterations: int = 4000, surface_points: int = 128,
+            wake_points: int = 65, normal_points: int = 97, first_layer_height: float = 1e-5,
+            upstream_chords: float = 10.0, downstream_chords: float = 15.0,
+            vertical_chords: float = 10.0, speed: float = 1.0, density: float = 1.0,
+            settings: Settings | None = None) -> Request:
+    r = Request()
+    r.designation = designation.encode()[:8]
+    r.grid_surface_points, r.grid_wake_points, r.grid_normal_points = surface_points, wake_points, normal_points
+    r.grid_first_layer_height = first_layer_height
+    r.grid_upstream_chords, r.grid_downstream_chords, r.grid_vertical_chords = (
+        upstream_chords, downstream_chords, vertical_chords)
+    r.alpha_deg, r.reynolds, r.speed, r.density = alpha_deg, reynolds, speed, density
+    r.model, r.tolerance, r.max_iterations = model, tolerance, max_iterations
+    r.settings = settings if settings is not None else Settings.defaults()
+    return r
+
+
+class Engine:
+    """Continuous batching of many solves (cfd_engine_*)."""
+
+    def __init__(self, memory_budget_bytes: int = 0, chunk: int = 32):
+        self._h = C.c_void_p()
+        _check(_lib.cfd_engine_create(memory_budget_bytes, chunk, C.byref(self._h)))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.cfd_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, req: Request) -> int:
+        out = C.c_int()
+        _check(_lib.cfd_engine_submit(self._h, C.byref(req), C.byref(out)))
+        return out.value
+
+    def step(self) -> tuple[int, int]:
+        a, q = C.c_int(), C.c_int()
+        _check(_lib.cfd_engine_step(self._h, C.byref(a), C.byref(q)))
+        return a.value, q.value
+
+    def results(self, capacity: int = 4096) -> list[Result]:
+        buf = (Result * capacity)()
+        count = C.c_int()
+        _check(_lib.cfd_engine_results(self._h, buf, capacity, C.byref(count)))
+        return [buf[k] for k in range(count.value)]
+
+    def clock(self) -> float:
+        return float(_lib.cfd_engine_clock(self._h))
+
+    def run(self, requests: list[Request]) -> list[Result]:
+        """Submit everything, step until the engine is empty."""
+        for r in requests:
+            self.submit(r)
+        out = []
+        while True:
+            active, queued = self.step()
+            out.extend(self.results())
+            if active == 0 and queued == 0:
+                break
+        out.extend(self.results())
+        return sorted(out, key=lambda r: r.id)
 
 
 def library_symbols() -> list[str]:

@@ -1,0 +1,414 @@
+// engine.cu - continuous batching of many SIMPLE solves on one GPU.
+//
+// A request queue feeds a set of resident solves. Each step admits queued
+// requests whose device footprint fits the memory budget, advances every
+// resident solve by up to `chunk` iterations in as few launches as there are
+// cluster shapes (one thread-block cluster per solve, each on its own
+// descriptor), then reads all monitors back with one copy and retires the
+// solves that finished. Retiring integrates the forces on the device and
+// frees the solve's memory, so the queue can fill it on the next step.
+//
+// The stop rules are the reference worker's (src/app/SolverWorker.cpp:164-192):
+// converged when worst() of the residuals drops below the tolerance,
+// diverged on a non-finite residual, iteration limit at the cap. A diverged
+// solve is restarted once from the freestream, as the polar sweep's
+// RetryCold does (src/post/Polar.cpp:109-121).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "cfd_gpu.h"
+#include "cfd_mesh.h"
+#include "common.hpp"
+#include "instance.hpp"
+#include "solver.hpp"
+
+namespace cfdb {
+
+Status makeCGrid(const char* designation, const cfd_cgrid_options& o, HostMesh* out);
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846;  // the double std::numbers::pi rounds to
+
+struct Slot {
+  int id{0};
+  cfd_request request{};
+  std::unique_ptr<Solver> solver;
+  int iterations{0};
+  bool retried{false};
+  double submitted{0.0}, started{0.0};
+  std::size_t bytes{0};
+};
+
+struct Pending {
+  int id{0};
+  cfd_request request{};
+  std::shared_ptr<const HostMesh> mesh;
+  double submitted{0.0};
+};
+
+using MeshKey = std::tuple<std::string, int, int, int, double, double, double, double>;
+
+MeshKey keyOf(const cfd_request& r) {
+  return {std::string(r.designation, strnlen(r.designation, sizeof(r.designation))),
+          r.grid_surface_points, r.grid_wake_points, r.grid_normal_points,
+          r.grid_first_layer_height, r.grid_upstream_chords, r.grid_downstream_chords,
+          r.grid_vertical_chords};
+}
+
+}  // namespace
+
+struct Engine {
+  std::size_t budget{0};
+  std::size_t used{0};
+  int chunk{32};
+  int nextId{0};
+  std::deque<Pending> queue;
+  std::vector<std::unique_ptr<Slot>> active;
+  std::vector<cfd_result> done;
+  std::map<MeshKey, std::shared_ptr<const HostMesh>> meshes;
+  std::chrono::steady_clock::time_point t0{std::chrono::steady_clock::now()};
+  // device status area: per slot, chunk monitors then the iteration count
+  double* dStatus{nullptr};
+  int statusSlots{0};
+  Instance* dTable{nullptr};
+  int tableSlots{0};
+  std::vector<cudaStream_t> streams;
+
+  double now() const {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  ~Engine() {
+    active.clear();
+    if (dStatus) cudaFree(dStatus);
+    if (dTable) cudaFree(dTable);
+    for (cudaStream_t s : streams) cudaStreamDestroy(s);
+  }
+
+  Status reserve(int slots) {
+    if (slots > statusSlots) {
+      if (dStatus) cudaFree(dStatus);
+      const int cap = std::max(slots, 2 * statusSlots);
+      const std::size_t per = static_cast<std::size_t>(chunk) * kMonSlots + 1;
+      if (cudaMalloc(reinterpret_cast<void**>(&dStatus), cap * per * sizeof(double)) != cudaSuccess) {
+        dStatus = nullptr;
+        statusSlots = 0;
+        return fail(CFD_INITIALIZATION_FAILURE, "engine status allocation failed");
+      }
+      statusSlots = cap;
+    }
+    if (slots > tableSlots) {
+      if (dTable) cudaFree(dTable);
+      const int cap = std::max(slots, 2 * tableSlots);
+      if (cudaMalloc(reinterpret_cast<void**>(&dTable), cap * sizeof(Instance)) != cudaSuccess) {
+        dTable = nullptr;
+        tableSlots = 0;
+        return fail(CFD_INITIALIZATION_FAILURE, "engine table allocation failed");
+      }
+      tableSlots = cap;
+    }
+    return ok();
+  }
+
+  static void uniform(const cfd_request& r, int cells, std::vector<double>* u, std::vector<double>* v,
+                      std::vector<double>* p, std::vector<double>* rho, std::vector<double>* mu) {
+    // FlowField::uniform (FlowField.cpp:21-47) with chord 1
+    const double alpha = r.alpha_deg * kPi / 180.0;
+    u->assign(cells, r.speed * std::cos(alpha));
+    v->assign(cells, r.speed * std::sin(alpha));
+    p->assign(cells, 0.0);
+    rho->assign(cells, r.density);
+    mu->assign(cells, r.density * r.speed * 1.0 / r.reynolds);
+  }
+
+  Status start(const Pending& q, std::unique_ptr<Slot>* out) {
+    const HostMesh& m = *q.mesh;
+    cfd_mesh_desc d;
+    describe(m, &d);
+    // buildFaceConditions with the default BoundaryConditions
+    std::vector<int> kind(m.faces);
+    std::vector<double> vel(2 * m.faces, 0.0), pres(m.faces, 0.0);
+    const double alpha = q.request.alpha_deg * kPi / 180.0;
+    const double ux = q.request.speed * std::cos(alpha), uy = q.request.speed * std::sin(alpha);
+    for (int f = 0; f < m.faces; ++f) {
+      int k = CFD_BC_INTERNAL;
+      if (m.boundary[f] == CFD_FACE_WALL) k = CFD_BC_NOSLIP_WALL;
+      else if (m.boundary[f] == CFD_FACE_FARFIELD) k = CFD_BC_FARFIELD;
+      else if (m.boundary[f] == CFD_FACE_OUTLET) k = CFD_BC_OUTLET;
+      kind[f] = k;
+      if (k != CFD_BC_NOSLIP_WALL) {
+        vel[2 * f] = ux;
+        vel[2 * f + 1] = uy;
+      }
+    }
+    cfd_face_bc bc{kind.data(), vel.data(), pres.data()};
+    Solver* raw = nullptr;
+    if (Status st = Solver::create(d, bc, fromC(q.request.settings), &raw); st != CFD_OK) return st;
+    std::unique_ptr<Solver> solver(raw);
+    if (Status st = solver->setTurbulence(q.request.model); st != CFD_OK) return st;
+    std::vector<double> u, v, p, rho, mu;
+    uniform(q.request, m.cells, &u, &v, &p, &rho, &mu);
+    if (Status st = solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()); st != CFD_OK) {
+      return st;
+    }
+    auto slot = std::make_unique<Slot>();
+    slot->id = q.id;
+    slot->request = q.request;
+    slot->bytes = solver->deviceBytes();
+    slot->solver = std::move(solver);
+    slot->submitted = q.submitted;
+    slot->started = now();
+    *out = std::move(slot);
+    return ok();
+  }
+
+  Status admit() {
+    while (!queue.empty()) {
+      const Pending& q = queue.front();
+      const std::size_t need = Solver::estimateBytes(q.mesh->nodesI - 1, q.mesh->nodesJ - 1);
+      // always admit into an empty engine, so one oversized request cannot stall the queue
+      if (!active.empty() && used + need > budget) break;
+      std::unique_ptr<Slot> slot;
+      if (Status st = start(q, &slot); st != CFD_OK) {
+        // a request that cannot start is reported, not retried
+        cfd_result r{};
+        r.id = q.id;
+        r.status = CFD_SOLVE_DIVERGED;
+        r.submitted_s = q.submitted;
+        r.started_s = r.finished_s = now();
+        done.push_back(r);
+        queue.pop_front();
+        continue;
+      }
+      used += slot->bytes;
+      active.push_back(std::move(slot));
+      queue.pop_front();
+    }
+    return ok();
+  }
+
+  void finish(Slot& s, int status, const double* mon) {
+    cfd_result r{};
+    r.id = s.id;
+    r.status = status;
+    r.iterations = s.iterations;
+    r.retried_cold = s.retried ? 1 : 0;
+    r.cells = s.solver->cells();
+    r.continuity = mon[kMonContinuity];
+    r.momentum_x = mon[kMonMomX];
+    r.momentum_y = mon[kMonMomY];
+    double f[10];
+    if (status != CFD_SOLVE_DIVERGED &&
+        s.solver->forces(s.request.speed, s.request.alpha_deg, s.request.density, 0.0, 1.0, f, nullptr,
+                         nullptr, nullptr, nullptr) == CFD_OK) {
+      r.lift_coefficient = f[0];
+      r.drag_coefficient = f[1];
+      r.moment_coefficient = f[2];
+      r.pressure_drag_coefficient = f[3];
+      r.friction_drag_coefficient = f[4];
+    }
+    r.submitted_s = s.submitted;
+    r.started_s = s.started;
+    r.finished_s = now();
+    done.push_back(r);
+  }
+
+  Status step(int* activeOut, int* queuedOut) {
+    if (Status st = admit(); st != CFD_OK) return st;
+    const int n = static_cast<int>(active.size());
+    if (n > 0) {
+      if (Status st = reserve(n); st != CFD_OK) return st;
+      // group by launch shape; table rows in slot order within each group
+      std::map<std::pair<int, int>, std::vector<int>> groups;
+      for (int k = 0; k < n; ++k) {
+        const Solver& s = *active[k]->solver;
+        groups[{s.clusterSize(), s.threads()}].push_back(k);
+      }
+      std::vector<Instance> table(n);
+      std::vector<std::tuple<int, int, int, int, int>> launches;  // offset, count, R, T, smem
+      const std::size_t per = static_cast<std::size_t>(chunk) * kMonSlots + 1;
+      int offset = 0;
+      for (const auto& [shape, members] : groups) {
+        int smem = 0;
+        for (std::size_t m = 0; m < members.size(); ++m) {
+          const int k = members[m];
+          Slot& s = *active[k];
+          Instance I = s.solver->deviceView();
+          double* status = dStatus + static_cast<std::size_t>(k) * per;
+          I.history = status;
+          I.iterations = reinterpret_cast<int*>(status + static_cast<std::size_t>(chunk) * kMonSlots);
+          I.stopTol = s.request.tolerance;
+          I.iterLimit = std::max(1, std::min(chunk, s.request.max_iterations - s.iterations));
+          table[offset + static_cast<int>(m)] = I;
+          smem = std::max(smem, cgSharedBytes(s.solver->cellsI(), s.solver->cellsJ(), shape.first));
+        }
+        launches.emplace_back(offset, static_cast<int>(members.size()), shape.first, shape.second, smem);
+        offset += static_cast<int>(members.size());
+      }
+      if (cudaMemcpy(dTable, table.data(), n * sizeof(Instance), cudaMemcpyHostToDevice) != cudaSuccess) {
+        return fail(CFD_INITIALIZATION_FAILURE, "engine table upload failed");
+      }
+      while (streams.size() < launches.size()) {
+        cudaStream_t s;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+          return fail(CFD_INITIALIZATION_FAILURE, "engine stream creation failed");
+        }
+        streams.push_back(s);
+      }
+      for (std::size_t g = 0; g < launches.size(); ++g) {
+        const auto [off, count, R, T, smem] = launches[g];
+        if (Status st = launchSimple(dTable + off, count, R, T, chunk, kStageEnd, -1.0, streams[g], smem);
+            st != CFD_OK) {
+          return st;
+        }
+      }
+      if (cudaDeviceSynchronize() != cudaSuccess) {
+        return fail(CFD_INITIALIZATION_FAILURE, "engine step failed on the device");
+      }
+      std::vector<double> status(static_cast<std::size_t>(n) * per);
+      if (cudaMemcpy(status.data(), dStatus, status.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
+          cudaSuccess) {
+        return fail(CFD_INITIALIZATION_FAILURE, "engine status read failed");
+      }
+      std::vector<std::unique_ptr<Slot>> keep;
+      for (int k = 0; k < n; ++k) {
+        Slot& s = *active[k];
+        const double* st = status.data() + static_cast<std::size_t>(k) * per;
+        int ran = 0;
+        std::memcpy(&ran, st + static_cast<std::size_t>(chunk) * kMonSlots, sizeof(int));
+        s.iterations += ran;
+        const double* mon = st + static_cast<std::size_t>(std::max(ran, 1) - 1) * kMonSlots;
+        const double a = mon[kMonContinuity], b = mon[kMonMomX], c = mon[kMonMomY];
+        const bool finite = std::isfinite(a) && std::isfinite(b) && std::isfinite(c);
+        int outcome = -1;
+        if (!finite) {
+          if (!s.retried) {
+            // RetryCold: restart once from the freestream
+            s.retried = true;
+            std::vector<double> u, v, p, rho, mu;
+            uniform(s.request, s.solver->cells(), &u, &v, &p, &rho, &mu);
+            if (s.solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()) != CFD_OK) {
+              outcome = CFD_SOLVE_DIVERGED;
+            }
+          } else {
+            outcome = CFD_SOLVE_DIVERGED;
+          }
+        } else if (std::max({std::abs(a), std::abs(b), std::abs(c)}) < s.request.tolerance) {
+          outcome = CFD_SOLVE_CONVERGED;
+        } else if (s.iterations >= s.request.max_iterations) {
+          outcome = CFD_SOLVE_ITERATION_LIMIT;
+        }
+        if (outcome >= 0) {
+          finish(s, outcome, mon);
+          used -= s.bytes;
+        } else {
+          keep.push_back(std::move(active[k]));
+        }
+      }
+      active = std::move(keep);
+    }
+    if (activeOut) *activeOut = static_cast<int>(active.size());
+    if (queuedOut) *queuedOut = static_cast<int>(queue.size());
+    return ok();
+  }
+};
+
+}  // namespace cfdb
+
+struct cfd_engine_t {
+  cfdb::Engine engine;
+};
+
+extern "C" {
+
+cfd_status cfd_engine_create(unsigned long long budget, int chunk, cfd_engine* out) {
+  if (out == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null output");
+  if (chunk < 1 || chunk > 256) return cfdb::fail(CFD_OUT_OF_RANGE, "chunk must lie in 1..256");
+  if (budget == 0) {
+    std::size_t freeBytes = 0, total = 0;
+    if (cudaMemGetInfo(&freeBytes, &total) != cudaSuccess) {
+      return cfdb::fail(CFD_INITIALIZATION_FAILURE, "cannot query device memory");
+    }
+    budget = static_cast<unsigned long long>(0.8 * static_cast<double>(freeBytes));
+  }
+  auto* e = new cfd_engine_t;
+  e->engine.budget = budget;
+  e->engine.chunk = chunk;
+  *out = e;
+  return CFD_OK;
+}
+
+cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* r, int* id) {
+  if (e == nullptr || r == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  if (!(r->reynolds > 0.0) || !(r->speed > 0.0) || !(r->density > 0.0) || !(r->tolerance >= 0.0) ||
+      r->max_iterations < 1 || (r->model != 0 && r->model != 1 && r->model != 2)) {
+    return cfdb::fail(CFD_INVALID_ARGUMENT, "invalid request");
+  }
+  cfdb::Engine& g = e->engine;
+  const cfdb::MeshKey key = cfdb::keyOf(*r);
+  auto it = g.meshes.find(key);
+  std::shared_ptr<const cfdb::HostMesh> mesh;
+  if (it != g.meshes.end()) {
+    mesh = it->second;
+  } else {
+    auto m = std::make_shared<cfdb::HostMesh>();
+    cfd_cgrid_options o;
+    cfd_default_cgrid_options(&o);
+    o.surface_points = r->grid_surface_points;
+    o.wake_points = r->grid_wake_points;
+    o.normal_points = r->grid_normal_points;
+    o.first_layer_height = r->grid_first_layer_height;
+    o.upstream_chords = r->grid_upstream_chords;
+    o.downstream_chords = r->grid_downstream_chords;
+    o.vertical_chords = r->grid_vertical_chords;
+    char name[9] = {0};
+    std::memcpy(name, r->designation, 8);
+    if (cfd_status st = cfdb::makeCGrid(name, o, m.get()); st != CFD_OK) return st;
+    mesh = m;
+    g.meshes[key] = mesh;
+  }
+  cfdb::Pending q;
+  q.id = g.nextId++;
+  q.request = *r;
+  q.mesh = mesh;
+  q.submitted = g.now();
+  g.queue.push_back(q);
+  if (id != nullptr) *id = q.id;
+  return CFD_OK;
+}
+
+cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued) {
+  if (e == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null engine");
+  return e->engine.step(active, queued);
+}
+
+cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* count) {
+  if (e == nullptr || count == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  cfdb::Engine& g = e->engine;
+  const int n = std::min<int>(capacity, static_cast<int>(g.done.size()));
+  for (int k = 0; k < n; ++k) out[k] = g.done[k];
+  g.done.erase(g.done.begin(), g.done.begin() + n);
+  *count = n;
+  return CFD_OK;
+}
+
+double cfd_engine_clock(cfd_engine e) { return (e == nullptr) ? 0.0 : e->engine.now(); }
+
+cfd_status cfd_engine_destroy(cfd_engine e) {
+  delete e;
+  return CFD_OK;
+}
+
+}  // extern "C"

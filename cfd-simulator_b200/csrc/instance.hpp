@@ -104,6 +104,10 @@ struct Instance {
   // ---- outputs ----
   double* history;   // kMonSlots doubles per iteration of the launch
   int* iterations;   // iterations completed by the launch
+
+  // ---- per-solve limits of a launch (batches and the engine) ----
+  double stopTol;    // convergence tolerance when the launch gives none (< 0: none)
+  int iterLimit;     // at most this many iterations in a launch
 };
 
 }  // namespace cfdb

@@ -1095,7 +1095,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
   const bool leader = (t.rank == 0 && t.tid == 0);
 
   int done = 0;
-  for (int it = 0; it < iterations; ++it) {
+  const int limit = (I.iterLimit < iterations) ? I.iterLimit : iterations;
+  const double stopTol = (tolerance >= 0.0) ? tolerance : I.stopTol;
+  for (int it = 0; it < limit; ++it) {
     double mon[kMonSlots];
 #pragma unroll
     for (int s = 0; s < kMonSlots; ++s) mon[s] = 0.0;
@@ -1318,10 +1320,10 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       for (int s = 0; s < kMonSlots; ++s) I.history[it * kMonSlots + s] = mon[s];
     }
     done = it + 1;
-    if (tolerance >= 0.0) {
+    if (stopTol >= 0.0) {
       const double a = mon[kMonContinuity], b = mon[kMonMomX], cc = mon[kMonMomY];
       if (!isfinite(a) || !isfinite(b) || !isfinite(cc)) break;
-      if (smax(smax(fabs(a), fabs(b)), fabs(cc)) < tolerance) break;
+      if (smax(smax(fabs(a), fabs(b)), fabs(cc)) < stopTol) break;
     }
   }
   if (leader) *I.iterations = done;

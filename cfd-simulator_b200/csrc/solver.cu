@@ -328,6 +328,7 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     dForces_ = a.take<double>(16);
   };
   carve(arena_);
+  arenaBytes_ = arena_.bytes();
   if (Status st = arena_.allocate(); st != CFD_OK) return st;
   carve(arena_);
   dHistory_ = view_.history;
@@ -419,6 +420,14 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
   return uploadSettings();
 }
 
+std::size_t Solver::estimateBytes(int NI, int NJ) {
+  // cell arrays (~60), face arrays of both families (~26), per-face geometry
+  // and conditions; rounded up generously.
+  const std::size_t N = static_cast<std::size_t>(NI) * NJ;
+  const std::size_t F = static_cast<std::size_t>(NI) * (NJ + 1) + static_cast<std::size_t>(NI + 1) * NJ;
+  return (64 * N + 16 * F) * 8 + (1u << 20);
+}
+
 Solver::~Solver() {
   if (stream_ != nullptr) cudaStreamDestroy(stream_);
 }
@@ -447,6 +456,8 @@ Status Solver::uploadSettings() {
   I.gamma1 = beta1 / betaStar - 0.5 * kappa * kappa / std::sqrt(betaStar);
   I.gamma2 = beta2 / betaStar - 0.856 * kappa * kappa / std::sqrt(betaStar);
   I.betaStarQuarter = std::pow(betaStar, 0.25);
+  I.stopTol = -1.0;
+  I.iterLimit = 0x7fffffff;
   CUDA_OR_FAIL(cudaMemcpy(dView_, &view_, sizeof(Instance), cudaMemcpyHostToDevice));
   return CFD_OK;
 }

@@ -95,6 +95,9 @@ class Solver {
   int clusterSize() const { return clusterSize_; }
   bool initialised() const { return initialised_; }
   int threads() const { return threads_; }
+  std::size_t deviceBytes() const { return arenaBytes_; }
+  /// Rough device footprint of a solve of NI x NJ cells (the arena's layout).
+  static std::size_t estimateBytes(int NI, int NJ);
   const Instance& deviceView() const { return view_; }
   cudaStream_t stream() const { return stream_; }
 
@@ -133,6 +136,7 @@ class Solver {
   double* dForces_{nullptr};
 
   DeviceArena arena_;
+  std::size_t arenaBytes_{0};
   Instance view_{};
   Instance* dView_{nullptr};
   double* dHistory_{nullptr};

@@ -254,6 +254,61 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
 cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double tolerance,
                                 int max_iterations, double* report, void* stream);
 
+/* ---- the solve engine: continuous batching of many solves ------------------
+ * A request loop over one GPU (no counterpart in the reference, which runs one
+ * solve per worker thread; its polar sweep runs points one after another,
+ * src/post/Polar.cpp:86-124). Requests queue until their device memory fits
+ * the budget; admitted solves stay resident, and every engine step advances
+ * all of them together (one launch per cluster shape, one thread-block
+ * cluster per solve, `chunk` iterations). A solve retires when its residuals
+ * pass the tolerance (converged), go non-finite (diverged: restarted once
+ * from the freestream, as the reference's RetryCold) or reach its iteration
+ * cap; its forces are integrated on the device and its memory freed for the
+ * queue. */
+typedef struct cfd_engine_t* cfd_engine;
+
+typedef struct cfd_request {
+  char designation[8];           /* NACA four digits, e.g. "2412" */
+  int grid_surface_points, grid_wake_points, grid_normal_points;
+  double grid_first_layer_height;
+  double grid_upstream_chords, grid_downstream_chords, grid_vertical_chords;
+  double alpha_deg, reynolds, speed, density;
+  int model;                     /* 0 laminar, 2 k-omega SST */
+  double tolerance;              /* worst() of the residuals */
+  int max_iterations;
+  cfd_settings settings;
+} cfd_request;
+
+enum { CFD_SOLVE_CONVERGED = 0, CFD_SOLVE_ITERATION_LIMIT = 1, CFD_SOLVE_DIVERGED = 2 };
+
+typedef struct cfd_result {
+  int id;
+  int status;                    /* CFD_SOLVE_* (pointStatus, Polar.cpp:79-84) */
+  int iterations;
+  int retried_cold;
+  int cells;
+  int pad_;
+  double continuity, momentum_x, momentum_y;
+  double lift_coefficient, drag_coefficient, moment_coefficient;
+  double pressure_drag_coefficient, friction_drag_coefficient;
+  double submitted_s, started_s, finished_s;  /* engine clock, seconds */
+} cfd_result;
+
+/* memory_budget_bytes: device memory the resident solves may hold (0: 80 %
+ * of the free memory). chunk: iterations per engine step. */
+cfd_status cfd_engine_create(unsigned long long memory_budget_bytes, int chunk, cfd_engine* out);
+/* Queue a request; *id identifies its result. Meshes are generated here. */
+cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* request, int* id);
+/* One step: admit what fits, advance every resident solve by up to `chunk`
+ * iterations, retire finished ones. active/queued (may be NULL) report the
+ * counts afterwards. */
+cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued);
+/* Move up to `capacity` finished results into `out`; *count gets how many. */
+cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* count);
+/* Seconds on the engine clock (for submit-time bookkeeping by callers). */
+double cfd_engine_clock(cfd_engine e);
+cfd_status cfd_engine_destroy(cfd_engine e);
+
 /* ---- batches: many solves in one launch ------------------------------------
  * A batch is a descriptor table over existing handles (each keeps its own
  * device state). One launch runs every solve of the table, one thread-block

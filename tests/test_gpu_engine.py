@@ -1,0 +1,88 @@
+"""The solve engine (continuous batching, cfd_engine_*): results alone and in
+a mix are the same, results equal a direct solve, admission respects the
+memory budget, and a diverging solve is retried cold once (Polar.cpp:109-121)
+and then reported diverged."""
+import numpy as np
+import pytest
+
+import cfd_b200 as cb
+
+pytestmark = pytest.mark.gpu
+
+TINY = dict(surface_points=24, wake_points=12, normal_points=13, first_layer_height=1e-4)
+
+
+def _req(designation="0012", alpha=4.0, re=1e6, model=cb.MODEL_SST, tol=1e-8, cap=3000, **kw):
+    grid = dict(TINY)
+    grid.update(kw.pop("grid", {}))
+    return cb.request(designation, alpha, re, model=model, tolerance=tol, max_iterations=cap,
+                      settings=cb.Settings.defaults(inflow_viscosity_ratio=10.0), **grid, **kw)
+
+
+def _key(r):
+    return (r.status, r.iterations, r.lift_coefficient, r.drag_coefficient, r.moment_coefficient)
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix():
+    mix = [_req(alpha=4.0), _req("2412", alpha=6.0, re=3e6),
+           _req(alpha=2.0, re=500.0, model=cb.MODEL_NONE, grid=dict(first_layer_height=2e-3)),
+           _req("0015", alpha=-3.0, re=2e5, grid=dict(surface_points=20, wake_points=8, normal_points=9))]
+    together = cb.Engine(chunk=16).run(mix)
+    assert [r.id for r in together] == list(range(len(mix)))
+    for k, req in enumerate(mix):
+        alone = cb.Engine(chunk=16).run([req])
+        a, b = alone[0], together[k]
+        assert a.status == b.status == 0, (a.status, b.status)
+        assert a.iterations == b.iterations
+        for x, y in ((a.lift_coefficient, b.lift_coefficient), (a.drag_coefficient, b.drag_coefficient),
+                     (a.moment_coefficient, b.moment_coefficient)):
+            assert x == pytest.approx(y, rel=1e-12, abs=1e-15)
+
+
+def test_engine_result_equals_a_direct_solve():
+    req = _req(alpha=4.0)
+    res = cb.Engine(chunk=32).run([req])[0]
+    mesh = cb.cgrid("0012", **TINY)
+    s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0),
+                               cb.Settings.defaults(inflow_viscosity_ratio=10.0))
+    s.set_turbulence_model(cb.MODEL_SST)
+    s.initialise(*cb.uniform_field(mesh, 1.0, 4.0, 1.0, 1e6))
+    taken, mon = s.converge(3000, 1e-8)
+    f, _, _ = s.forces(1.0, 4.0, 1.0)
+    assert res.status == 0 and res.iterations == taken
+    assert res.lift_coefficient == pytest.approx(f.lift_coefficient, rel=1e-12)
+    assert res.drag_coefficient == pytest.approx(f.drag_coefficient, rel=1e-12)
+    assert res.continuity == pytest.approx(mon.continuity, rel=1e-12)
+
+
+def test_admission_by_memory_budget_runs_one_at_a_time():
+    engine = cb.Engine(memory_budget_bytes=1, chunk=64)  # room for one resident solve
+    for alpha in (0.0, 2.0, 4.0):
+        engine.submit(_req(alpha=alpha, tol=1e-6))
+    results, peak = [], 0
+    while True:
+        active, queued = engine.step()
+        peak = max(peak, active)
+        results.extend(engine.results())
+        if active == 0 and queued == 0:
+            break
+    assert peak == 1
+    assert sorted(r.id for r in results) == [0, 1, 2]
+    assert all(r.status == 0 for r in results)
+    starts = sorted(r.started_s for r in results)
+    ends = sorted(r.finished_s for r in results)
+    assert starts[1] >= ends[0] and starts[2] >= ends[1]
+
+
+def test_a_diverging_solve_is_retried_cold_once_then_reported():
+    bad = cb.Settings.defaults(velocity_relaxation=1.0, pressure_relaxation=1.0)
+    req = cb.request("0012", 8.0, 1e6, model=cb.MODEL_NONE, tolerance=1e-8, max_iterations=2000,
+                     settings=bad, **TINY)
+    r = cb.Engine(chunk=16).run([req])[0]
+    assert r.status == 2 and r.retried_cold == 1
+    assert not np.isfinite(r.continuity) or not np.isfinite(r.momentum_x)
+
+
+def test_iteration_limit_is_reported():
+    r = cb.Engine(chunk=16).run([_req(tol=1e-30, cap=40)])[0]
+    assert r.status == 1 and r.iterations == 40
