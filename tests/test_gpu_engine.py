@@ -44,7 +44,8 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
 def test_engine_result_equals_a_direct_solve():
     req = _req(alpha=4.0)
     res = cb.Engine(chunk=32).run([req])[0]
-    mesh = cb.cgrid("0012", **TINY)
+    mesh = cb.cgrid("0012", upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0,
+                    **TINY)
     s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0),
                                cb.Settings.defaults(inflow_viscosity_ratio=10.0))
     s.set_turbulence_model(cb.MODEL_SST)
