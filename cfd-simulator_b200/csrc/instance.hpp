@@ -53,6 +53,7 @@ enum Stage : int {
 // Kernel implementation flags (bit mask).
 constexpr int kFlagGlobalCg = 1;
 constexpr int kFlagPlainWavefront = 2;
+constexpr int kFlagSequentialRows = 4;
 
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {

@@ -465,10 +465,10 @@ DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
   q = eq * wq;
 }
 
-/// Lexicographic Gauss-Seidel sweeps of one system (LinearSystem.cpp:77-116)
-/// computed row by row. With row j-1 already updated and row j+1 and the
-/// east neighbours still holding their old values, the cell-order update of
-/// row j is the first-order recurrence x_i = p_i + q_i x_{i-1},
+/// One row of a lexicographic Gauss-Seidel sweep (LinearSystem.cpp:77-116).
+/// With row j-1 already updated and row j+1 and the east neighbours still
+/// holding their old values, the cell-order update of row j is the
+/// first-order recurrence x_i = p_i + q_i x_{i-1},
 ///   p_i = (b_i - aS x_S - aE x_E - aN x_N) / a_P,  q_i = -aW / a_P,
 /// solved by a block-wide scan. Row 0 is split in two: the wake-cut partner
 /// (NI-1-i, 0) of (i, 0) comes later in the row for i < NI/2 (old value) and
@@ -476,76 +476,117 @@ DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
 /// first. A cell with a_P = 0 keeps its value (p = x, q = 0). This is the
 /// reference's sweep map; only the rounding differs from cell-by-cell order.
 ///
-/// Run by every thread of one CTA. Needs NI <= 8 * blockDim.x and
-/// 2 * NI + 2 * warps doubles of shared memory.
-DEV void gsRowScanSweeps(const Instance& I, int sweeps, const double* D, const double* cS,
-                         const double* cN, const double* cW, const double* cE, const double* b,
-                         double* x, double* smem) {
+/// Run by every thread of one CTA; rowPrev holds row j-1's new values and
+/// receives row j's. Needs NI <= 8 * blockDim.x. Ends without a barrier after
+/// the row is published (the caller synchronises before the next row).
+DEV void gsRow(const Instance& I, int j, const double* D, const double* cS, const double* cN,
+               const double* cW, const double* cE, const double* b, double* x, double* rowNew,
+               double* rowPrev, double* sc) {
   const int NI = I.NI, NJ = I.NJ;
   const int T = blockDim.x;
   const int per = (NI + T - 1) / T;  // contiguous cells per thread
-  double* rowNew = smem;             // row j, new values
-  double* rowPrev = smem + NI;       // row j - 1, new values
-  double* sc = smem + 2 * NI;
   const int i0 = threadIdx.x * per;
+  const int segments = (j == 0) ? 2 : 1;
+  double carry = 0.0;
+  for (int seg = 0; seg < segments; ++seg) {
+    const int lo = (segments == 1) ? 0 : (seg == 0 ? 0 : NI / 2);
+    const int hi = (segments == 1) ? NI : (seg == 0 ? NI / 2 : NI);
+    double pv[8], qv[8];
+    double P = 0.0, Q = 1.0;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      pv[e] = 0.0;
+      qv[e] = 1.0;
+      const int i = i0 + e;
+      if (e >= per || i < lo || i >= hi) continue;
+      const int c = j * NI + i;
+      const double d = D[c];
+      if (!(fabs(d) > 0.0)) {
+        pv[e] = x[c];
+        qv[e] = 0.0;
+      } else {
+        double off = 0.0;
+        if (j > 0) {
+          off += cS[c] * rowPrev[i];
+        } else {
+          const int a = I.acrossJ0[i];
+          if (a >= 0) off += cS[c] * ((a < i) ? rowNew[a] : x[a]);
+        }
+        if (i < NI - 1) off += cE[c] * x[c + 1];
+        if (j < NJ - 1) off += cN[c] * x[c + NI];
+        pv[e] = (b[c] - off) / d;
+        qv[e] = (i > 0) ? -cW[c] / d : 0.0;
+      }
+      P = pv[e] + qv[e] * P;
+      Q = qv[e] * Q;
+    }
+    blockAffineExclusiveScan(P, Q, sc);
+    double xv = P + Q * carry;  // value entering this thread's chunk
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int i = i0 + e;
+      if (e >= per || i < lo || i >= hi) continue;
+      xv = pv[e] + qv[e] * xv;
+      rowNew[i] = xv;
+    }
+    __syncthreads();
+    if (hi > lo) carry = rowNew[hi - 1];
+  }
+  // Publish row j: global memory (east/north reads of later rows and the
+  // next sweep) and rowPrev (the south values of row j + 1). Every read of
+  // this row's old values and of rowPrev happened before the scan's barriers
+  // above.
+  for (int i = threadIdx.x; i < NI; i += T) {
+    x[j * NI + i] = rowNew[i];
+    rowPrev[i] = rowNew[i];
+  }
+}
+
+/// `sweeps` lexicographic sweeps of one system by one CTA, row after row.
+/// Needs 2 * NI + 2 * warps doubles of shared memory.
+DEV void gsRowScanSweeps(const Instance& I, int sweeps, const double* D, const double* cS,
+                         const double* cN, const double* cW, const double* cE, const double* b,
+                         double* x, double* smem) {
+  double* rowNew = smem;        // row j, new values
+  double* rowPrev = smem + I.NI;  // row j - 1, new values
+  double* sc = smem + 2 * I.NI;
   for (int sweep = 0; sweep < sweeps; ++sweep) {
-    for (int j = 0; j < NJ; ++j) {
-      const int segments = (j == 0) ? 2 : 1;
-      double carry = 0.0;
-      for (int seg = 0; seg < segments; ++seg) {
-        const int lo = (segments == 1) ? 0 : (seg == 0 ? 0 : NI / 2);
-        const int hi = (segments == 1) ? NI : (seg == 0 ? NI / 2 : NI);
-        double pv[8], qv[8];
-        double P = 0.0, Q = 1.0;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          pv[e] = 0.0;
-          qv[e] = 1.0;
-          const int i = i0 + e;
-          if (e >= per || i < lo || i >= hi) continue;
-          const int c = j * NI + i;
-          const double d = D[c];
-          if (!(fabs(d) > 0.0)) {
-            pv[e] = x[c];
-            qv[e] = 0.0;
-          } else {
-            double off = 0.0;
-            if (j > 0) {
-              off += cS[c] * rowPrev[i];
-            } else {
-              const int a = I.acrossJ0[i];
-              if (a >= 0) off += cS[c] * ((a < i) ? rowNew[a] : x[a]);
-            }
-            if (i < NI - 1) off += cE[c] * x[c + 1];
-            if (j < NJ - 1) off += cN[c] * x[c + NI];
-            pv[e] = (b[c] - off) / d;
-            qv[e] = (i > 0) ? -cW[c] / d : 0.0;
-          }
-          P = pv[e] + qv[e] * P;
-          Q = qv[e] * Q;
-        }
-        blockAffineExclusiveScan(P, Q, sc);
-        double xv = P + Q * carry;  // value entering this thread's chunk
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int i = i0 + e;
-          if (e >= per || i < lo || i >= hi) continue;
-          xv = pv[e] + qv[e] * xv;
-          rowNew[i] = xv;
-        }
-        __syncthreads();
-        if (hi > lo) carry = rowNew[hi - 1];
-      }
-      // Publish row j: global memory (east/north reads of later rows and the
-      // next sweep) and rowPrev (the south values of row j + 1). Every read
-      // of this row's old values and of rowPrev happened before the scan's
-      // barriers above.
-      for (int i = threadIdx.x; i < NI; i += T) {
-        x[j * NI + i] = rowNew[i];
-        rowPrev[i] = rowNew[i];
-      }
+    for (int j = 0; j < I.NJ; ++j) {
+      gsRow(I, j, D, cS, cN, cW, cE, b, x, rowNew, rowPrev, sc);
       __syncthreads();
     }
+  }
+}
+
+/// The k and omega sweeps as a software pipeline over 2 * sweeps CTAs: CTA
+/// (eq, s) runs sweep s of equation eq (0: k, 1: omega) and at step t updates
+/// row t - 2s. Sweep s reads row j+1 as left by sweep s-1 (done at step t-1),
+/// row j as left by sweep s-1 (step t-2) and row j-1 from its own previous
+/// step, so every value is the one the sequential order would use, and no row
+/// is written at the step it is read by another sweep (sweep s-1 writes row
+/// j+2, sweep s+1 row j-2). Every CTA of the cluster joins each step's
+/// barrier. Same arithmetic as gsRowScanSweeps, NJ + 2 (sweeps - 1) steps
+/// instead of sweeps * NJ.
+DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, double* smem) {
+  const int role = static_cast<int>(t.rank);
+  const bool active = role < 2 * sweeps;
+  const bool omega = active && role >= sweeps;
+  const int s = active ? role % sweeps : 0;
+  const double* D = omega ? I.wD : I.kD;
+  const double* cS = omega ? I.wS : I.kS;
+  const double* cN = omega ? I.wN : I.kN;
+  const double* cW = omega ? I.wW : I.kW;
+  const double* cE = omega ? I.wE : I.kE;
+  const double* b = omega ? I.wB : I.kB;
+  double* x = omega ? I.om : I.k;
+  double* rowNew = smem;
+  double* rowPrev = smem + I.NI;
+  double* sc = smem + 2 * I.NI;
+  const int steps = I.NJ + 2 * (sweeps - 1);
+  for (int step = 0; step < steps; ++step) {
+    const int j = step - 2 * s;
+    if (active && j >= 0 && j < I.NJ) gsRow(I, j, D, cS, cN, cW, cE, b, x, rowNew, rowPrev, sc);
+    t.cl.sync();
   }
 }
 
@@ -1277,11 +1318,14 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       // state depends on the order (a colouring would move it by ~1e-3).
       if (!(flags & kFlagPlainWavefront) && I.NI <= 8 * t.T &&
           (2 * I.NI + 64) * 8 <= smemBytes) {
-        // rank 0 sweeps k, rank 1 omega (one CTA: both, one after the other)
-        if (t.R == 1) {
+        if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
+          gsRowScanPipelined(I, t, 3, dyn);
+        } else if (t.R == 1) {
+          // one CTA: k, then omega
           gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
           gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
         } else if (t.rank == 0) {
+          // rank 0 sweeps k, rank 1 omega
           gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
         } else if (t.rank == 1) {
           gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
@@ -1370,12 +1414,10 @@ int chooseClusterSize(int cells) {
 int kernelFlags() {
   // Implementation choices for tuning comparisons (results are identical):
   // bit 0 keeps the pressure CG in global memory, bit 1 uses the plain
-  // wavefront sweeps.
-  static const int flags = [] {
-    const char* env = std::getenv("CFD_KERNEL_FLAGS");
-    return (env != nullptr) ? std::atoi(env) : 0;
-  }();
-  return flags;
+  // wavefront sweeps, bit 2 runs the k/omega row sweeps one after another
+  // instead of pipelined across CTAs.
+  const char* env = std::getenv("CFD_KERNEL_FLAGS");
+  return (env != nullptr) ? std::atoi(env) : 0;
 }
 
 int cgSharedBytes(int NI, int NJ, int clusterSize) {
