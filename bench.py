@@ -398,15 +398,8 @@ def _summarise(results, wall_s, cb):
             "iterations": _percentiles([r.iterations for r in results])}
 
 
-def run_polar(args) -> None:
-    """configs[3]: 21-point NACA 2412 SST Re 3e6 polar (alpha -4..16 step 1) on
-    the fine 768x192 C-grid, plus NACA 0012 SST Re 1e6 alpha 4 on the coarse,
-    medium and fine grids, all resident at once in one engine."""
-    import torch
-    torch.cuda.set_device(0)
-    import cfd_b200 as cb
-    cb.set_device(0)
-    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO)
+def _polar_requests(cb, args, precision):
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO, precision=precision)
     reqs = []
     for alpha in range(-4, 17):
         s, w, n = GRIDS["fine"]
@@ -418,19 +411,59 @@ def run_polar(args) -> None:
         reqs.append(cb.request("0012", 4.0, 1e6, tolerance=args.tolerance, max_iterations=args.cap,
                                surface_points=s, wake_points=w, normal_points=n,
                                first_layer_height=fl, settings=settings))
-    engine = cb.Engine(chunk=args.chunk)
-    t0 = time.perf_counter()
-    results = engine.run(reqs)
-    wall = time.perf_counter() - t0
-    out = _summarise(results, wall, cb)
-    out.update({"workload": "polar: NACA2412 SST Re3e6 768x192 alpha -4..16 + NACA0012 SST Re1e6 "
-                            "alpha 4 on 192x48/384x96/768x192", "tolerance": args.tolerance,
-                "cap": args.cap, "chunk": args.chunk,
-                "polar": [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
-                           "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
-                           "iterations": r.iterations, "cl": r.lift_coefficient,
-                           "cd": r.drag_coefficient, "cm": r.moment_coefficient,
-                           "continuity": r.continuity} for r in results]})
+    return reqs
+
+
+def run_polar(args) -> None:
+    """configs[3]: 21-point NACA 2412 SST Re 3e6 polar (alpha -4..16 step 1) on
+    the fine 768x192 C-grid, plus NACA 0012 SST Re 1e6 alpha 4 on the coarse,
+    medium and fine grids, all resident at once in one engine; run in the
+    plain FP64 form and in the mixed FP32/FP64 form, with the mixed answers'
+    differences from the FP64 ones (Cl, Cd, Cm, and Cp at every station)."""
+    import torch
+    torch.cuda.set_device(0)
+    import cfd_b200 as cb
+    cb.set_device(0)
+    forms = ("plain", "mixed") if args.precision == "both" else (args.precision,)
+    out = {"workload": "polar: NACA2412 SST Re3e6 768x192 alpha -4..16 + NACA0012 SST Re1e6 "
+                       "alpha 4 on 192x48/384x96/768x192", "tolerance": args.tolerance,
+           "cap": args.cap, "chunk": args.chunk}
+    runs = {}
+    for form in forms:
+        reqs = _polar_requests(cb, args, 0 if form == "plain" else 1)
+        engine = cb.Engine(chunk=args.chunk)
+        t0 = time.perf_counter()
+        results = sorted(engine.run(reqs), key=lambda r: r.id)
+        wall = time.perf_counter() - t0
+        cps = {r.id: engine.surface(r.id) for r in results if r.status != 2}
+        engine.close()
+        runs[form] = (results, cps)
+        summary = _summarise(results, wall, cb)
+        summary["polar"] = [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
+                             "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
+                             "iterations": r.iterations, "cl": r.lift_coefficient,
+                             "cd": r.drag_coefficient, "cm": r.moment_coefficient,
+                             "continuity": r.continuity} for r in results]
+        out[form] = summary
+    if len(forms) == 2:
+        (rp, cpp), (rm, cpm) = runs["plain"], runs["mixed"]
+        rows = []
+        for a, b in zip(rp, rm):
+            row = {"id": a.id, "dcl": abs(b.lift_coefficient - a.lift_coefficient),
+                   "dcd": abs(b.drag_coefficient - a.drag_coefficient),
+                   "dcm": abs(b.moment_coefficient - a.moment_coefficient),
+                   "iterations_plain": a.iterations, "iterations_mixed": b.iterations}
+            if a.id in cpp and b.id in cpm and len(cpp[a.id]) == len(cpm[b.id]):
+                row["dcp_inf"] = float(np.max(np.abs(cpm[b.id] - cpp[a.id])))
+            rows.append(row)
+        both_converged = [r for r, a, b in zip(rows, rp, rm) if a.status == 0 and b.status == 0]
+        out["mixed_vs_plain"] = {
+            "solves_per_min_ratio": out["mixed"]["solves_per_min"] / out["plain"]["solves_per_min"],
+            "max_dcl": max(r["dcl"] for r in rows), "max_dcd": max(r["dcd"] for r in rows),
+            "max_dcm": max(r["dcm"] for r in rows),
+            "max_dcp_inf": max((r.get("dcp_inf", 0.0) for r in rows), default=None),
+            "max_dcl_both_converged": max((r["dcl"] for r in both_converged), default=None),
+            "per_solve": rows}
     print(json.dumps(out), flush=True)
 
 
@@ -457,7 +490,8 @@ def run_serve(args) -> None:
     import cfd_b200 as cb
     cb.set_device(0)
     stream = serving_stream(args.requests, args.rate, args.seed)
-    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO)
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO,
+                                    precision=1 if args.precision == "mixed" else 0)
     engine = cb.Engine(chunk=args.chunk)
     t0 = engine.clock()
     submitted, results = 0, []
@@ -479,7 +513,8 @@ def run_serve(args) -> None:
     out = _summarise(results, wall, cb)
     out.update({"workload": f"serve: Poisson lambda={args.rate}/s, {args.requests} NACA 4-digit SST "
                             f"requests (seed {args.seed}), meshes 192x48/384x96/768x192 at "
-                            "0.5/0.35/0.15", "tolerance": args.tolerance, "cap": args.cap,
+                            "0.5/0.35/0.15", "precision": args.precision if args.precision == "mixed" else "plain",
+                "tolerance": args.tolerance, "cap": args.cap,
                 "chunk": args.chunk})
     print(json.dumps(out), flush=True)
 
@@ -499,6 +534,8 @@ def main() -> None:
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--precision", choices=("plain", "mixed", "both"), default="both",
+                    help="polar: which form(s) to run; serve: plain unless 'mixed'")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

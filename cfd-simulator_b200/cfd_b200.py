@@ -192,6 +192,7 @@ _sig("cfd_engine_create", C.c_int, C.c_ulonglong, C.c_int, _P)
 _sig("cfd_engine_submit", C.c_int, _P, _P, _P)
 _sig("cfd_engine_step", C.c_int, _P, _P, _P)
 _sig("cfd_engine_results", C.c_int, _P, _P, C.c_int, _P)
+_sig("cfd_engine_surface", C.c_int, _P, C.c_int, _P, C.c_int, _P)
 _sig("cfd_engine_clock", C.c_double, _P)
 _sig("cfd_engine_destroy", C.c_int, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
@@ -541,7 +542,7 @@ class Request(C.Structure):
 
 class Result(C.Structure):
     _fields_ = [("id", C.c_int), ("status", C.c_int), ("iterations", C.c_int),
-                ("retried_cold", C.c_int), ("cells", C.c_int), ("pad_", C.c_int),
+                ("retried_cold", C.c_int), ("cells", C.c_int), ("cluster_size", C.c_int),
                 ("continuity", C.c_double), ("momentum_x", C.c_double),
                 ("momentum_y", C.c_double), ("lift_coefficient", C.c_double),
                 ("drag_coefficient", C.c_double), ("moment_coefficient", C.c_double),
@@ -550,7 +551,7 @@ class Result(C.Structure):
                 ("started_s", C.c_double), ("finished_s", C.c_double)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad_"}
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 STATUS_NAMES = {0: "converged", 1: "iteration-limit", 2: "diverged"}
@@ -607,6 +608,14 @@ class Engine:
         count = C.c_int()
         _check(_lib.cfd_engine_results(self._h, buf, capacity, C.byref(count)))
         return [buf[k] for k in range(count.value)]
+
+    def surface(self, request_id: int) -> np.ndarray:
+        """Cp per wall station of a finished solve (taken once)."""
+        n = C.c_int()
+        _check(_lib.cfd_engine_surface(self._h, request_id, None, 0, C.byref(n)))
+        cp = np.zeros(n.value)
+        _check(_lib.cfd_engine_surface(self._h, request_id, _ptr(cp), n.value, C.byref(n)))
+        return cp
 
     def clock(self) -> float:
         return float(_lib.cfd_engine_clock(self._h))

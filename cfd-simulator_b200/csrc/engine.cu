@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -77,7 +78,9 @@ struct Engine {
   std::deque<Pending> queue;
   std::vector<std::unique_ptr<Slot>> active;
   std::vector<cfd_result> done;
+  std::map<int, std::vector<double>> surfaces;  // Cp per wall station of each finished solve
   std::map<MeshKey, std::shared_ptr<const HostMesh>> meshes;
+  std::map<std::tuple<int, int, int, int>, std::pair<int, int>> shapes;  // tuned launch shapes
   std::chrono::steady_clock::time_point t0{std::chrono::steady_clock::now()};
   // device status area: per slot, chunk monitors then the iteration count
   double* dStatus{nullptr};
@@ -134,6 +137,69 @@ struct Engine {
   }
 
   Status start(const Pending& q, std::unique_ptr<Slot>* out) {
+    std::unique_ptr<Solver> solver;
+    if (Status st = makeSolver(q, &solver); st != CFD_OK) return st;
+    std::pair<int, int> shape;
+    if (Status st = tunedShape(q, *solver, &shape); st != CFD_OK) return st;
+    if (Status st = solver->setLaunchShape(shape.first, shape.second); st != CFD_OK) return st;
+    auto slot = std::make_unique<Slot>();
+    slot->id = q.id;
+    slot->request = q.request;
+    slot->bytes = solver->deviceBytes();
+    slot->solver = std::move(solver);
+    slot->submitted = q.submitted;
+    slot->started = now();
+    *out = std::move(slot);
+    return ok();
+  }
+
+  /// The launch shape of a grid: among clusters of 4, 6, 8 and 16 CTAs of 512
+  /// threads, the one that gives the most solve-iterations per second on a
+  /// full GPU, (clusters resident at once) / (time per iteration), timed on
+  /// a scratch solve of the same grid, model and precision from its uniform
+  /// start. Chosen once per (cells I, cells J, model, precision) and cached,
+  /// so a request runs with the same shape, and gives the same bits, whatever
+  /// else is in the engine. CFD_ENGINE_TUNE=0 keeps the solver's default.
+  Status tunedShape(const Pending& q, const Solver& s, std::pair<int, int>* out) {
+    const auto key = std::make_tuple(s.cellsI(), s.cellsJ(), q.request.model, s.precision());
+    if (auto it = shapes.find(key); it != shapes.end()) {
+      *out = it->second;
+      return ok();
+    }
+    std::pair<int, int> best{s.clusterSize(), s.threads()};
+    const char* env = std::getenv("CFD_ENGINE_TUNE");
+    if (env == nullptr || std::atoi(env) != 0) {
+      std::unique_ptr<Solver> probe;
+      if (Status st = makeSolver(q, &probe); st != CFD_OK) return st;
+      double bestScore = -1.0;
+      for (int R : {4, 6, 8, 16}) {
+        if (R > s.cellsJ()) continue;
+        const int T = 512;
+        if (probe->setLaunchShape(R, T) != CFD_OK) continue;
+        const int resident = maxActiveClusters(R, T, probe->launchSmemBytes(R));
+        if (resident <= 0) continue;
+        std::vector<double> u, v, p, rho, mu;
+        uniform(q.request, probe->cells(), &u, &v, &p, &rho, &mu);
+        if (probe->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()) != CFD_OK) continue;
+        int taken = 0;
+        if (probe->iterate(3, kStageEnd, -1.0, nullptr, &taken) != CFD_OK) continue;
+        const auto t0 = std::chrono::steady_clock::now();
+        if (probe->iterate(8, kStageEnd, -1.0, nullptr, &taken) != CFD_OK) continue;
+        const double perIteration =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / 8.0;
+        const double score = resident / perIteration;
+        if (score > bestScore) {
+          bestScore = score;
+          best = {R, T};
+        }
+      }
+    }
+    shapes[key] = best;
+    *out = best;
+    return ok();
+  }
+
+  Status makeSolver(const Pending& q, std::unique_ptr<Solver>* out) {
     const HostMesh& m = *q.mesh;
     cfd_mesh_desc d;
     describe(m, &d);
@@ -163,14 +229,7 @@ struct Engine {
     if (Status st = solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()); st != CFD_OK) {
       return st;
     }
-    auto slot = std::make_unique<Slot>();
-    slot->id = q.id;
-    slot->request = q.request;
-    slot->bytes = solver->deviceBytes();
-    slot->solver = std::move(solver);
-    slot->submitted = q.submitted;
-    slot->started = now();
-    *out = std::move(slot);
+    *out = std::move(solver);
     return ok();
   }
 
@@ -206,13 +265,18 @@ struct Engine {
     r.iterations = s.iterations;
     r.retried_cold = s.retried ? 1 : 0;
     r.cells = s.solver->cells();
+    r.cluster_size = s.solver->clusterSize();
     r.continuity = mon[kMonContinuity];
     r.momentum_x = mon[kMonMomX];
     r.momentum_y = mon[kMonMomY];
     double f[10];
+    std::vector<double> cp(static_cast<std::size_t>(std::max(s.solver->wallStations(), 1)));
+    int stations = 0;
     if (status != CFD_SOLVE_DIVERGED &&
-        s.solver->forces(s.request.speed, s.request.alpha_deg, s.request.density, 0.0, 1.0, f, nullptr,
-                         nullptr, nullptr, nullptr) == CFD_OK) {
+        s.solver->forces(s.request.speed, s.request.alpha_deg, s.request.density, 0.0, 1.0, f, cp.data(),
+                         nullptr, &stations, nullptr) == CFD_OK) {
+      cp.resize(static_cast<std::size_t>(stations));
+      surfaces[s.id] = std::move(cp);
       r.lift_coefficient = f[0];
       r.drag_coefficient = f[1];
       r.moment_coefficient = f[2];
@@ -252,7 +316,7 @@ struct Engine {
           I.stopTol = s.request.tolerance;
           I.iterLimit = std::max(1, std::min(chunk, s.request.max_iterations - s.iterations));
           table[offset + static_cast<int>(m)] = I;
-          smem = std::max(smem, cgSharedBytes(s.solver->cellsI(), s.solver->cellsJ(), shape.first));
+          smem = std::max(smem, s.solver->launchSmemBytes(shape.first));
         }
         launches.emplace_back(offset, static_cast<int>(members.size()), shape.first, shape.second, smem);
         offset += static_cast<int>(members.size());
@@ -401,6 +465,20 @@ cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* 
   for (int k = 0; k < n; ++k) out[k] = g.done[k];
   g.done.erase(g.done.begin(), g.done.begin() + n);
   *count = n;
+  return CFD_OK;
+}
+
+cfd_status cfd_engine_surface(cfd_engine e, int id, double* cp, int capacity, int* stations) {
+  if (e == nullptr || stations == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  cfdb::Engine& g = e->engine;
+  auto it = g.surfaces.find(id);
+  if (it == g.surfaces.end()) return cfdb::fail(CFD_INVALID_ARGUMENT, "no surface data for this request id");
+  const int n = static_cast<int>(it->second.size());
+  *stations = n;
+  if (cp == nullptr) return CFD_OK;  // size query
+  if (capacity < n) return cfdb::fail(CFD_INVALID_ARGUMENT, "cp buffer too small");
+  std::copy(it->second.begin(), it->second.end(), cp);
+  g.surfaces.erase(it);
   return CFD_OK;
 }
 

@@ -62,9 +62,46 @@ enum MonitorSlot : int {
   kMonMaxW, kMonMinMut, kMonMaxMut, kMonMaxRatio, kMonMaxYPlus, kMonSlots
 };
 
+// ---- mixed form: the pressure-correction multigrid -----------------------------
+
+constexpr int kMaxMgLevels = 12;
+
+/// One level of the pressure-correction multigrid: a cellsI x cellsJ block
+/// with a five-point row per cell, cell c = j*NI + i as on the fine grid.
+/// Level l+1 aggregates 2 x 2 cells of level l (the top row alone when NJ is
+/// odd) and its rows are the Galerkin sums of the fine rows. The wake cut
+/// carries over: on every level column i at j = 0 couples to wake[i].
+struct MgLevel {
+  int NI, NJ;
+  float *D, *S, *N, *W, *E;  // row coefficients (global memory)
+  float* inv;                // 1 / D (0 where D = 0)
+  float *x, *b;              // iterate and right-hand side (global memory)
+  const int* wake;           // partner column across j = 0, or -1
+  int smem;                  // byte offset of the level in shared memory when rank 0 runs it alone
+};
+
+struct Multigrid {
+  int levels;       // >= 1
+  int distributed;  // levels 0 .. distributed-1 are split over the cluster in row bands
+  int warpFrom;     // levels warpFrom .. levels-1 (64 cells or fewer) run on rank 0's warp 0
+  int pre, post, coarse;  // Gauss-Seidel sweeps (red-black) per level and on the coarsest
+  int smemBytes;    // shared memory of the levels rank 0 runs alone
+  MgLevel lv[kMaxMgLevels];
+  // inner flexible-CG vectors, FP32, fine-grid layout
+  float *r, *q, *e, *z0, *z1, *d0, *d1;
+};
+
+/// FP32 rows of one system in correction form, A delta = r: the mixed form
+/// sweeps delta in FP32 from zero and adds it to the FP64 unknowns.
+struct Rows32 {
+  float *D, *S, *N, *W, *E;  // row coefficients
+  float *r, *x;              // residual b - A phi (from FP64) and the correction
+};
+
 struct Instance {
   int NI, NJ, N;
   int model;  // 0 none, 1 laminar closure, 2 k-omega SST
+  int precision;  // 0 plain FP64, 1 mixed FP32/FP64
 
   // ---- settings (SimpleSettings) ----
   double alphaU, alphaP, blend, alphaT;
@@ -105,6 +142,12 @@ struct Instance {
   // ---- outputs ----
   double* history;   // kMonSlots doubles per iteration of the launch
   int* iterations;   // iterations completed by the launch
+
+  // ---- mixed form ----
+  Multigrid mg;
+  Rows32 mom;          // momentum rows (shared by u and v); r, x belong to u
+  float *momRv, *momXv;  // v's residual and correction
+  Rows32 tk, tw;       // k and omega
 
   // ---- per-solve limits of a launch (batches and the engine) ----
   double stopTol;    // convergence tolerance when the launch gives none (< 0: none)

@@ -1,0 +1,578 @@
+// pressure_mg.cuh - the mixed form's pressure-correction solve (included by
+// simple_kernel.cu inside its anonymous namespace).
+//
+// The plain form runs the reference's Jacobi-PCG (LinearSystem.cpp:118-210)
+// and, at its cap of 200 iterations, reduces the L1 residual of the p'
+// system by only ~2.5x on a 384x96 C-grid (it would need ~1000 iterations
+// for the reference's 1% target). The mixed form solves the same system to
+// the same stopping rule (sum |r| <= tol * sum |r0|, at most `cgMax`
+// iterations) with a stronger inner solver:
+//
+//   outer (FP64):  x = 0, r = b;  repeat: inner solve A e = r in FP32,
+//                  x += e, r = b - A x (FP64 rows), stop on the L1 rule.
+//   inner (FP32):  flexible CG (Polak-Ribiere beta, dot products and norms
+//                  accumulated in FP64) preconditioned by one multigrid
+//                  V-cycle per iteration.
+//   V-cycle:       2x2 aggregation with Galerkin rows, so every level is a
+//                  five-point block with the wake-cut map carried over;
+//                  red-black Gauss-Seidel (red then black going down, black
+//                  then red coming up, so the cycle is symmetric); the
+//                  fine levels are split over the cluster in row bands with a
+//                  cluster barrier per half sweep, the coarse levels (a few
+//                  thousand cells) run on rank 0 alone from shared memory
+//                  with __syncthreads only, and the last few (64 cells or
+//                  fewer) on its warp 0 with __syncwarp.
+//
+// Fusions that save barriers: the red half sweep of a level from a zero
+// start is x = b / D and is written by whatever phase produced b; the
+// prolongation is folded into the first post-smoothing half sweep (a black
+// cell needs only its red neighbours' corrected values, and every red value
+// is recomputed by the following red half sweep); the last red half sweep on
+// the fine level is fused with the CG's reduction.
+
+/// A level as the code sees it: coefficient and vector pointers in global or
+/// shared memory.
+struct Lv {
+  int NI, NJ;
+  float *D, *S, *N, *W, *E, *inv, *x, *b;
+  const int* wake;
+};
+
+/// The rows [j0, j1) of a level that one worker set covers: a row band of
+/// the cluster, all of a level for the CTA that runs it alone, or all of it
+/// for one warp.
+struct Span {
+  int j0, j1, tid, T;
+};
+
+DEV Lv globalLevel(const MgLevel& M) {
+  return Lv{M.NI, M.NJ, M.D, M.S, M.N, M.W, M.E, M.inv, M.x, M.b, M.wake};
+}
+
+/// Eight arrays of the level in shared memory from byte offset M.smem, each
+/// rounded up to 4 floats.
+DEV Lv sharedLevel(const MgLevel& M, char* smem) {
+  float* p = reinterpret_cast<float*>(smem + M.smem);
+  const int n = (M.NI * M.NJ + 3) & ~3;
+  return Lv{M.NI, M.NJ, p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, p + 6 * n, p + 7 * n, M.wake};
+}
+
+DEV Lv levelView(const Instance& I, int l, char* smem) {
+  const MgLevel& M = I.mg.lv[l];
+  return (l < I.mg.distributed) ? globalLevel(M) : sharedLevel(M, smem);
+}
+
+DEV Span bandOf(const Lv& L, const Team& t) {
+  const int R = static_cast<int>(t.R), r = static_cast<int>(t.rank);
+  return Span{(L.NJ * r) / R, (L.NJ * (r + 1)) / R, t.tid, t.T};
+}
+DEV Span wholeOf(const Lv& L) { return Span{0, L.NJ, static_cast<int>(threadIdx.x), static_cast<int>(blockDim.x)}; }
+DEV Span warpOf(const Lv& L) { return Span{0, L.NJ, static_cast<int>(threadIdx.x & 31), 32}; }
+
+/// f(c, i, j) for every cell of the span.
+template <typename F>
+DEV void forCells(const Lv& L, const Span& s, F&& f) {
+  const int count = (s.j1 - s.j0) * L.NI;
+  for (int m = s.tid; m < count; m += s.T) {
+    const int jj = m / L.NI;
+    const int i = m - jj * L.NI, j = s.j0 + jj;
+    f(j * L.NI + i, i, j);
+  }
+}
+
+/// f(c, i, j) for the cells of one colour ((i + j) & 1) of the span; with
+/// NI even every row holds NI / 2 of them.
+template <typename F>
+DEV void forColour(const Lv& L, const Span& s, int colour, F&& f) {
+  if ((L.NI & 1) == 0) {
+    const int half = L.NI >> 1;
+    const int count = (s.j1 - s.j0) * half;
+    for (int m = s.tid; m < count; m += s.T) {
+      const int jj = m / half;
+      const int j = s.j0 + jj;
+      const int i = 2 * (m - jj * half) + ((colour + j) & 1);
+      f(j * L.NI + i, i, j);
+    }
+  } else {
+    forCells(L, s, [&](int c, int i, int j) {
+      if (((i + j) & 1) == colour) f(c, i, j);
+    });
+  }
+}
+
+/// Off-diagonal part of row c applied to x (S, N, W, E).
+DEV float offSum(const Lv& L, const float* x, int c, int i, int j) {
+  float s = 0.0f;
+  if (j > 0) {
+    s += L.S[c] * x[c - L.NI];
+  } else {
+    const int a = L.wake[i];
+    if (a >= 0) s += L.S[c] * x[a];
+  }
+  if (j < L.NJ - 1) s += L.N[c] * x[c + L.NI];
+  if (i > 0) s += L.W[c] * x[c - 1];
+  if (i < L.NI - 1) s += L.E[c] * x[c + 1];
+  return s;
+}
+
+/// The same with every neighbour's value corrected by its aggregate's value
+/// on the next coarser level (piecewise-constant prolongation).
+DEV float offSumProlonged(const Lv& L, const float* ec, int NIc, int c, int i, int j) {
+  auto val = [&](int n, int ni, int nj) { return L.x[n] + ec[(nj >> 1) * NIc + (ni >> 1)]; };
+  float s = 0.0f;
+  if (j > 0) {
+    s += L.S[c] * val(c - L.NI, i, j - 1);
+  } else {
+    const int a = L.wake[i];
+    if (a >= 0) s += L.S[c] * val(a, a, 0);
+  }
+  if (j < L.NJ - 1) s += L.N[c] * val(c + L.NI, i, j + 1);
+  if (i > 0) s += L.W[c] * val(c - 1, i - 1, j);
+  if (i < L.NI - 1) s += L.E[c] * val(c + 1, i + 1, j);
+  return s;
+}
+
+/// Gauss-Seidel half sweep over the cells of one colour. Each thread takes
+/// up to four cells at a time and loads everything for them before it
+/// stores, so the loads of the four overlap (a store to x could otherwise
+/// alias the next cell's loads and serialise them).
+template <bool kProlonged>
+DEV void sweepCells(const Lv& L, const Span& s, int colour, const float* ec, int NIc) {
+  const int rows = s.j1 - s.j0;
+  if ((L.NI & 1) != 0) {
+    // the coarsest level may have an odd width: plain loop
+    forCells(L, s, [&](int c, int i, int j) {
+      if (((i + j) & 1) != colour) return;
+      const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
+      L.x[c] = (L.b[c] - off) * L.inv[c];
+    });
+    return;
+  }
+  const int half = L.NI >> 1;
+  const int count = rows * half;
+  for (int m0 = s.tid; m0 < count; m0 += 4 * s.T) {
+    float val[4];
+    int at[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int m = m0 + k * s.T;
+      at[k] = -1;
+      if (m < count) {
+        const int jj = m / half;
+        const int j = s.j0 + jj;
+        const int i = 2 * (m - jj * half) + ((colour + j) & 1);
+        const int c = j * L.NI + i;
+        const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
+        val[k] = (L.b[c] - off) * L.inv[c];
+        at[k] = c;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (at[k] >= 0) L.x[at[k]] = val[k];
+    }
+  }
+}
+
+DEV void colourSweep(const Lv& L, const Span& s, int colour) { sweepCells<false>(L, s, colour, nullptr, 0); }
+
+/// The black half sweep that opens post-smoothing, with the coarse
+/// correction ec (level above, NIc columns) added to the neighbours on the fly.
+DEV void colourSweepProlonged(const Lv& L, const Span& s, const float* ec, int NIc) {
+  sweepCells<true>(L, s, 1, ec, NIc);
+}
+
+/// Sum of the fine residual b - A x over the aggregate of coarse cell (I, J).
+DEV float aggregateResidual(const Lv& F, int I, int J) {
+  float sum = 0.0f;
+  for (int bj = 0; bj < 2; ++bj) {
+    const int jf = 2 * J + bj;
+    if (jf >= F.NJ) break;
+#pragma unroll
+    for (int ai = 0; ai < 2; ++ai) {
+      const int fi = 2 * I + ai, f = jf * F.NI + fi;
+      sum += F.b[f] - F.D[f] * F.x[f] - offSum(F, F.x, f, fi, jf);
+    }
+  }
+  return sum;
+}
+
+/// Restrict the fine residual b - A x to the coarse right-hand side (sum over
+/// each aggregate). With `start`, also begin the coarse level: red cells
+/// b / D, black 0. Four coarse cells per thread at a time, loads first.
+template <bool kStart>
+DEV void restrictCells(const Lv& F, const Lv& C, const Span& s) {
+  const int count = (s.j1 - s.j0) * C.NI;
+  for (int m0 = s.tid; m0 < count; m0 += 4 * s.T) {
+    float val[4];
+    int at[4], colour[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int m = m0 + k * s.T;
+      at[k] = -1;
+      if (m < count) {
+        const int jj = m / C.NI;
+        const int I = m - jj * C.NI, J = s.j0 + jj;
+        val[k] = aggregateResidual(F, I, J);
+        at[k] = J * C.NI + I;
+        colour[k] = (I + J) & 1;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (at[k] < 0) continue;
+      C.b[at[k]] = val[k];
+      if (kStart) C.x[at[k]] = (colour[k] == 0) ? val[k] * C.inv[at[k]] : 0.0f;
+    }
+  }
+}
+
+DEV void restrictInto(const Lv& F, const Lv& C, const Span& s) { restrictCells<true>(F, C, s); }
+
+/// Galerkin rows of the coarse level: P^T A P with P the 2x2 aggregation.
+/// Couplings inside an aggregate join the diagonal; the others are summed
+/// per side. Row 0's S couplings cross the wake cut to the partner aggregate.
+DEV void galerkin(const Lv& F, const Lv& C, const Span& s) {
+  forCells(C, s, [&](int cc, int I, int J) {
+    float D = 0.0f, S = 0.0f, N = 0.0f, W = 0.0f, E = 0.0f;
+    for (int bj = 0; bj < 2; ++bj) {
+      const int jf = 2 * J + bj;
+      if (jf >= F.NJ) break;
+#pragma unroll
+      for (int ai = 0; ai < 2; ++ai) {
+        const int fi = 2 * I + ai, f = jf * F.NI + fi;
+        D += F.D[f];
+        if (jf > 0) {
+          if (bj == 1) D += F.S[f]; else S += F.S[f];
+        } else if (F.wake[fi] >= 0) {
+          S += F.S[f];
+        }
+        if (jf < F.NJ - 1) {
+          if (bj == 0) D += F.N[f]; else N += F.N[f];
+        }
+        if (fi > 0) {
+          if (ai == 1) D += F.W[f]; else W += F.W[f];
+        }
+        if (fi < F.NI - 1) {
+          if (ai == 0) D += F.E[f]; else E += F.E[f];
+        }
+      }
+    }
+    C.D[cc] = D; C.S[cc] = S; C.N[cc] = N; C.W[cc] = W; C.E[cc] = E;
+    C.inv[cc] = (D != 0.0f) ? 1.0f / D : 0.0f;
+  });
+}
+
+/// The levels below `first` down to the coarsest, then back up to `first`,
+/// by one worker set that synchronises with `sync` (a CTA or a warp). On
+/// entry level `first` holds its right-hand side and its red start; on exit
+/// its x is final.
+template <typename Sync, typename SpanOf>
+DEV void localCycle(const Instance& I, char* smem, int first, Sync sync, SpanOf spanOf) {
+  const Multigrid& G = I.mg;
+  const int L = G.levels;
+  int l = first;
+  for (; l < L; ++l) {
+    const Lv A = sharedLevel(G.lv[l], smem);
+    const Span s = spanOf(A);
+    const bool coarsest = (l == L - 1);
+    const int sweeps = coarsest ? G.coarse : G.pre;
+    sync();
+    colourSweep(A, s, 1);
+    for (int k = 1; k < sweeps; ++k) {
+      sync();
+      colourSweep(A, s, 0);
+      sync();
+      colourSweep(A, s, 1);
+    }
+    if (coarsest) break;
+    sync();
+    const Lv C = sharedLevel(G.lv[l + 1], smem);
+    restrictInto(A, C, spanOf(C));
+  }
+  for (l = L - 2; l >= first; --l) {
+    const Lv A = sharedLevel(G.lv[l], smem);
+    const Lv C = sharedLevel(G.lv[l + 1], smem);
+    const Span s = spanOf(A);
+    for (int h = 0; h < 2 * G.post; ++h) {
+      sync();
+      if (h == 0) colourSweepProlonged(A, s, C.x, C.NI);
+      else colourSweep(A, s, (h & 1) ? 0 : 1);
+    }
+  }
+  sync();
+}
+
+/// Rank 0 alone: take the first shared-memory level's right-hand side (the
+/// cluster restricted it into global memory), run the V-cycle below it
+/// (levels of at most 64 cells on warp 0 alone), and publish that level's x
+/// to global memory for the cluster's prolongation.
+DEV void sharedCycle(const Instance& I, char* smem) {
+  const Multigrid& G = I.mg;
+  const int L = G.levels, m = G.distributed, w = G.warpFrom;
+  {
+    // the cluster restricted into level m's global right-hand side
+    const Lv C = sharedLevel(G.lv[m], smem);
+    const float* bg = G.lv[m].b;
+    forCells(C, wholeOf(C), [&](int c, int i, int j) {
+      const float b = bg[c];
+      C.b[c] = b;
+      C.x[c] = (((i + j) & 1) == 0) ? b * C.inv[c] : 0.0f;
+    });
+  }
+  auto block = [] { __syncthreads(); };
+  auto warp = [] { __syncwarp(); };
+  if (w == m) {
+    // every shared level is small: warp 0 runs them all
+    __syncthreads();
+    if (threadIdx.x < 32) localCycle(I, smem, m, warp, [](const Lv& A) { return warpOf(A); });
+  } else {
+    // block levels [m, w), then warp levels [w, L)
+    int l = m;
+    for (; l < w; ++l) {
+      const Lv A = sharedLevel(G.lv[l], smem);
+      const Span s = wholeOf(A);
+      const bool coarsest = (l == L - 1);
+      const int sweeps = coarsest ? G.coarse : G.pre;
+      __syncthreads();
+      colourSweep(A, s, 1);
+      for (int k = 1; k < sweeps; ++k) {
+        __syncthreads();
+        colourSweep(A, s, 0);
+        __syncthreads();
+        colourSweep(A, s, 1);
+      }
+      if (coarsest) break;
+      __syncthreads();
+      const Lv C = sharedLevel(G.lv[l + 1], smem);
+      restrictInto(A, C, wholeOf(C));
+    }
+    if (w < L) {
+      __syncthreads();
+      if (threadIdx.x < 32) localCycle(I, smem, w, warp, [](const Lv& A) { return warpOf(A); });
+    }
+    for (l = ((w < L) ? w : L - 1) - 1; l >= m; --l) {
+      const Lv A = sharedLevel(G.lv[l], smem);
+      const Lv C = sharedLevel(G.lv[l + 1], smem);
+      const Span s = wholeOf(A);
+      for (int h = 0; h < 2 * G.post; ++h) {
+        __syncthreads();
+        if (h == 0) colourSweepProlonged(A, s, C.x, C.NI);
+        else colourSweep(A, s, (h & 1) ? 0 : 1);
+      }
+    }
+  }
+  (void)block;
+  __syncthreads();
+  const Lv A = sharedLevel(G.lv[m], smem);
+  float* out = G.lv[m].x;
+  for (int c = threadIdx.x; c < A.NI * A.NJ; c += blockDim.x) out[c] = A.x[c];
+}
+
+/// z = M r, one V-cycle. On entry the fine level's red cells of z hold r / D
+/// and its black cells 0 (written by the caller's previous loop, before any
+/// barrier). On exit, after a cluster barrier, z is complete except for the
+/// last red half sweep on the fine level, which the caller fuses with its
+/// reduction.
+DEV void vcycle(const Instance& I, Team& t, char* smem, float* z) {
+  const Multigrid& G = I.mg;
+  const int L = G.levels, Ld = G.distributed;
+  auto view = [&](int l) {
+    Lv v = levelView(I, l, smem);
+    if (l == 0) {
+      v.x = z;
+      v.b = G.r;
+    }
+    return v;
+  };
+  for (int l = 0; l < Ld; ++l) {
+    const Lv F = view(l);
+    const Span s = bandOf(F, t);
+    const bool coarsest = (l == L - 1);
+    const int sweeps = coarsest ? G.coarse : G.pre;
+    t.cl.sync();
+    colourSweep(F, s, 1);
+    for (int k = 1; k < sweeps; ++k) {
+      t.cl.sync();
+      colourSweep(F, s, 0);
+      t.cl.sync();
+      colourSweep(F, s, 1);
+    }
+    if (coarsest) break;
+    t.cl.sync();
+    if (l + 1 < Ld) {
+      const Lv C = view(l + 1);
+      restrictInto(F, C, bandOf(C, t));
+    } else {
+      // every CTA restricts its band into the first shared level's global
+      // right-hand side; rank 0 then runs the levels below on its own
+      const Lv C = globalLevel(G.lv[l + 1]);
+      restrictCells<false>(F, C, bandOf(C, t));
+      t.cl.sync();
+      if (t.rank == 0) sharedCycle(I, smem);
+    }
+  }
+  for (int l = (Ld < L) ? Ld - 1 : L - 2; l >= 0; --l) {
+    const Lv F = view(l);
+    const Span s = bandOf(F, t);
+    const float* ec = G.lv[l + 1].x;  // coarse correction, global memory on every level
+    const int NIc = G.lv[l + 1].NI;
+    int halves = 2 * G.post;
+    if (l == 0) --halves;  // the caller's last red half sweep
+    for (int h = 0; h < halves; ++h) {
+      t.cl.sync();
+      if (h == 0) colourSweepProlonged(F, s, ec, NIc);
+      else colourSweep(F, s, (h & 1) ? 0 : 1);
+    }
+  }
+  t.cl.sync();
+}
+
+/// The pressure-correction solve of the mixed form. On entry I.x = 0 and
+/// I.r = I.pB (the caller's start of the CG); `initial` = sum |b|. Returns
+/// the inner iterations run (the monitor's pressure iterations).
+__device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh, double* dyn,
+                                          double initial) {
+  const Multigrid& G = I.mg;
+  char* smem = reinterpret_cast<char*>(dyn);
+  const int NI = I.NI, NJ = I.NJ;
+  const int op1[1] = {kSum};
+  const int op3[3] = {kSum, kSum, kSum};
+
+  // ---- set-up: the fine rows in FP32, then the Galerkin levels ----
+  const Lv F0 = globalLevel(G.lv[0]);
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % NI, j = c / NI;
+    F0.D[c] = static_cast<float>(I.pD[c]);
+    F0.S[c] = static_cast<float>((j > 0) ? I.pN[j * NI + i] : ((I.acrossJ0[i] >= 0) ? I.pN[i] : 0.0));
+    F0.N[c] = static_cast<float>((j < NJ - 1) ? I.pN[(j + 1) * NI + i] : 0.0);
+    F0.W[c] = static_cast<float>((i > 0) ? I.pE[j * (NI + 1) + i] : 0.0);
+    F0.E[c] = static_cast<float>((i < NI - 1) ? I.pE[j * (NI + 1) + i + 1] : 0.0);
+    F0.inv[c] = (F0.D[c] != 0.0f) ? 1.0f / F0.D[c] : 0.0f;
+  }
+  for (int l = 1; l < G.distributed; ++l) {
+    t.cl.sync();
+    const Lv C = levelView(I, l, smem);
+    galerkin(levelView(I, l - 1, smem), C, bandOf(C, t));
+  }
+  t.cl.sync();
+  if (G.distributed < G.levels && t.rank == 0) {
+    for (int l = G.distributed; l < G.levels; ++l) {
+      if (l > G.distributed) __syncthreads();
+      const Lv C = sharedLevel(G.lv[l], smem);
+      galerkin(levelView(I, l - 1, smem), C, wholeOf(C));
+    }
+    // the first V-cycle's barriers order these rows before their use
+  }
+
+  const double tolAbs = I.cgTol * initial;
+  float* r = G.r;
+  float* q = G.q;
+  float* e = G.e;
+  int total = 0;
+  for (int refine = 0; refine < 3 && total < I.cgMax; ++refine) {
+    // ---- inner solve of A e = r in FP32 ----
+    float* zc = G.z0;
+    float* zp = G.z1;
+    float* dc = G.d0;
+    float* dn = G.d1;
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % NI, j = c / NI;
+      const float rc = static_cast<float>(I.r[c]);
+      r[c] = rc;
+      e[c] = 0.0f;
+      zc[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
+    }
+    vcycle(I, t, smem, zc);
+    double rz;
+    {
+      Lv Z = F0;
+      Z.x = zc;
+      Z.b = r;
+      double v1[1] = {0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        const int i = c % NI, j = c / NI;
+        if (((i + j) & 1) == 0) zc[c] = (r[c] - offSum(Z, zc, c, i, j)) * Z.inv[c];
+        v1[0] += static_cast<double>(r[c]) * static_cast<double>(zc[c]);
+      }
+      teamReduce(t, sh, v1, op1);
+      rz = v1[0];
+    }
+    double beta = 0.0;
+    for (int it = 0; total < I.cgMax; ++it) {
+      // q = A d' with d' = z + beta d, formed for each cell and its neighbours.
+      double dq[1] = {0.0};
+      const float fb = static_cast<float>(beta);
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        const int i = c % NI, j = c / NI;
+        auto dir = [&](int n) { return (it == 0) ? zc[n] : zc[n] + fb * dc[n]; };
+        const float dv = dir(c);
+        dn[c] = dv;
+        float y = F0.D[c] * dv;
+        if (j > 0) {
+          y += F0.S[c] * dir(c - NI);
+        } else {
+          const int a = I.acrossJ0[i];
+          if (a >= 0) y += F0.S[c] * dir(a);
+        }
+        if (j < NJ - 1) y += F0.N[c] * dir(c + NI);
+        if (i > 0) y += F0.W[c] * dir(c - 1);
+        if (i < NI - 1) y += F0.E[c] * dir(c + 1);
+        q[c] = y;
+        dq[0] += static_cast<double>(dv) * static_cast<double>(y);
+      }
+      {
+        float* tmp = dc;
+        dc = dn;
+        dn = tmp;
+      }
+      teamReduce(t, sh, dq, op1);
+      if (!(fabs(dq[0]) > 0.0) || !isfinite(dq[0])) break;
+      const float alpha = static_cast<float>(rz / dq[0]);
+      double v3[3] = {0.0, 0.0, 0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        const int i = c % NI, j = c / NI;
+        e[c] += alpha * dc[c];
+        const float rc = r[c] - alpha * q[c];
+        r[c] = rc;
+        v3[2] += fabs(static_cast<double>(rc));
+        zp[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
+      }
+      ++total;
+      vcycle(I, t, smem, zp);
+      {
+        Lv Z = F0;
+        Z.x = zp;
+        Z.b = r;
+        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+          const int i = c % NI, j = c / NI;
+          if (((i + j) & 1) == 0) zp[c] = (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c];
+          const double rc = static_cast<double>(r[c]);
+          v3[0] += rc * static_cast<double>(zp[c]);
+          v3[1] += rc * static_cast<double>(zc[c]);
+        }
+      }
+      teamReduce(t, sh, v3, op3);
+      if (v3[2] <= tolAbs) break;
+      if (!(fabs(rz) > 0.0) || !isfinite(v3[0])) break;
+      beta = (v3[0] - v3[1]) / rz;  // Polak-Ribiere: stays a CG for a varying preconditioner
+      rz = v3[0];
+      float* tmp = zc;
+      zc = zp;
+      zp = tmp;
+    }
+    // ---- outer refinement in FP64: x += e, r = b - A x ----
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] += static_cast<double>(e[c]);
+    t.cl.sync();
+    double l1[1] = {0.0};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % NI, j = c / NI;
+      const double rc = I.pB[c] - pressureRow(I, c, i, j, I.x, I.x[c]);
+      I.r[c] = rc;
+      l1[0] += fabs(rc);
+    }
+    teamReduce(t, sh, l1, op1);
+    if (l1[0] <= tolAbs) break;
+  }
+  return total;
+}

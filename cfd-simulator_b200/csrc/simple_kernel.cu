@@ -314,6 +314,49 @@ DEV void phaseMomentum(const Instance& I, Team& t, double& resU, double& resV, d
     resU += fabs(sU - yu);
     resV += fabs(sV - yv);
     diagL1 += fabs(diag);
+    if (I.precision == 1) {
+      // FP32 rows and residuals for the correction-form sweeps.
+      const Rows32& m = I.mom;
+      m.D[c] = static_cast<float>(diag);
+      m.S[c] = static_cast<float>(off[0]);
+      m.N[c] = static_cast<float>(off[1]);
+      m.W[c] = static_cast<float>(off[2]);
+      m.E[c] = static_cast<float>(off[3]);
+      m.r[c] = static_cast<float>(sU - yu);
+      I.momRv[c] = static_cast<float>(sV - yv);
+      m.x[c] = 0.0f;
+      I.momXv[c] = 0.0f;
+    }
+  }
+}
+
+/// Mixed form: one red-black colour pass of the momentum corrections
+/// (A du = ru, A dv = rv in FP32, shared rows). The last pass of the last
+/// sweep also adds both corrections to the FP64 velocities of every own cell:
+/// the other colour's corrections are final by then and no neighbour reads u
+/// or v during the sweeps.
+DEV void gsColourMixed(const Instance& I, Team& t, int colour, bool last) {
+  const Rows32& m = I.mom;
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % I.NI, j = c / I.NI;
+    if (((i + j) & 1) == colour) {
+      const float d = m.D[c];
+      if (d != 0.0f) {
+        const int nS = across(I, c, i, j, 0), nN = across(I, c, i, j, 1);
+        const int nW = across(I, c, i, j, 2), nE = across(I, c, i, j, 3);
+        float ou = 0.0f, ov = 0.0f;
+        if (nS >= 0) { ou += m.S[c] * m.x[nS]; ov += m.S[c] * I.momXv[nS]; }
+        if (nE >= 0) { ou += m.E[c] * m.x[nE]; ov += m.E[c] * I.momXv[nE]; }
+        if (nN >= 0) { ou += m.N[c] * m.x[nN]; ov += m.N[c] * I.momXv[nN]; }
+        if (nW >= 0) { ou += m.W[c] * m.x[nW]; ov += m.W[c] * I.momXv[nW]; }
+        m.x[c] = (m.r[c] - ou) / d;
+        I.momXv[c] = (I.momRv[c] - ov) / d;
+      }
+    }
+    if (last) {
+      I.u[c] += static_cast<double>(m.x[c]);
+      I.v[c] += static_cast<double>(I.momXv[c]);
+    }
   }
 }
 
@@ -409,26 +452,27 @@ DEV void gsWavefrontSweeps(const Instance& I, Team& t, int sweeps, const double*
 /// order: each thread passes the composition (p, q) of its own elements
 /// (identity (0, 1) if none) and receives the composition of all elements of
 /// lower threads. Uses sc[0 .. 2*warps) of shared memory; two __syncthreads.
-DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
+template <typename T>
+DEV void blockAffineExclusiveScan(T& p, T& q, T* sc) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
   // inclusive scan within the warp (later maps applied after earlier ones)
-  double ip = p, iq = q;
+  T ip = p, iq = q;
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
-    const double pp = __shfl_up_sync(0xffffffffu, ip, off);
-    const double qq = __shfl_up_sync(0xffffffffu, iq, off);
+    const T pp = __shfl_up_sync(0xffffffffu, ip, off);
+    const T qq = __shfl_up_sync(0xffffffffu, iq, off);
     if (lane >= off) {
       ip = ip + iq * pp;
       iq = iq * qq;
     }
   }
   // exclusive within the warp
-  double ep = __shfl_up_sync(0xffffffffu, ip, 1);
-  double eq = __shfl_up_sync(0xffffffffu, iq, 1);
+  T ep = __shfl_up_sync(0xffffffffu, ip, 1);
+  T eq = __shfl_up_sync(0xffffffffu, iq, 1);
   if (lane == 0) {
-    ep = 0.0;
-    eq = 1.0;
+    ep = T(0);
+    eq = T(1);
   }
   if (lane == 31) {
     sc[2 * warp] = ip;
@@ -436,22 +480,22 @@ DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
   }
   __syncthreads();
   if (warp == 0) {
-    double wp = (lane < nwarps) ? sc[2 * lane] : 0.0;
-    double wq = (lane < nwarps) ? sc[2 * lane + 1] : 1.0;
+    T wp = (lane < nwarps) ? sc[2 * lane] : T(0);
+    T wq = (lane < nwarps) ? sc[2 * lane + 1] : T(1);
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-      const double pp = __shfl_up_sync(0xffffffffu, wp, off);
-      const double qq = __shfl_up_sync(0xffffffffu, wq, off);
+      const T pp = __shfl_up_sync(0xffffffffu, wp, off);
+      const T qq = __shfl_up_sync(0xffffffffu, wq, off);
       if (lane >= off) {
         wp = wp + wq * pp;
         wq = wq * qq;
       }
     }
-    double xp = __shfl_up_sync(0xffffffffu, wp, 1);
-    double xq = __shfl_up_sync(0xffffffffu, wq, 1);
+    T xp = __shfl_up_sync(0xffffffffu, wp, 1);
+    T xq = __shfl_up_sync(0xffffffffu, wq, 1);
     if (lane == 0) {
-      xp = 0.0;
-      xq = 1.0;
+      xp = T(0);
+      xq = T(1);
     }
     if (lane < nwarps) {
       sc[2 * lane] = xp;
@@ -460,7 +504,7 @@ DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
   }
   __syncthreads();
   // earlier warps first, then the earlier lanes of this warp
-  const double wp = sc[2 * warp], wq = sc[2 * warp + 1];
+  const T wp = sc[2 * warp], wq = sc[2 * warp + 1];
   p = ep + eq * wp;
   q = eq * wq;
 }
@@ -479,33 +523,40 @@ DEV void blockAffineExclusiveScan(double& p, double& q, double* sc) {
 /// Run by every thread of one CTA; rowPrev holds row j-1's new values and
 /// receives row j's. Needs NI <= 8 * blockDim.x. Ends without a barrier after
 /// the row is published (the caller synchronises before the next row).
-DEV void gsRow(const Instance& I, int j, const double* D, const double* cS, const double* cN,
-               const double* cW, const double* cE, const double* b, double* x, double* rowNew,
-               double* rowPrev, double* sc) {
+template <typename T>
+struct SysView {
+  const T *D, *S, *N, *W, *E, *b;
+  T* x;
+};
+
+template <typename T>
+DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowPrev, T* sc) {
+  const T *D = y.D, *cS = y.S, *cN = y.N, *cW = y.W, *cE = y.E, *b = y.b;
+  T* x = y.x;
   const int NI = I.NI, NJ = I.NJ;
-  const int T = blockDim.x;
-  const int per = (NI + T - 1) / T;  // contiguous cells per thread
+  const int nt = blockDim.x;
+  const int per = (NI + nt - 1) / nt;  // contiguous cells per thread
   const int i0 = threadIdx.x * per;
   const int segments = (j == 0) ? 2 : 1;
-  double carry = 0.0;
+  T carry = T(0);
   for (int seg = 0; seg < segments; ++seg) {
     const int lo = (segments == 1) ? 0 : (seg == 0 ? 0 : NI / 2);
     const int hi = (segments == 1) ? NI : (seg == 0 ? NI / 2 : NI);
-    double pv[8], qv[8];
-    double P = 0.0, Q = 1.0;
+    T pv[8], qv[8];
+    T P = T(0), Q = T(1);
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
-      pv[e] = 0.0;
-      qv[e] = 1.0;
+      pv[e] = T(0);
+      qv[e] = T(1);
       const int i = i0 + e;
       if (e >= per || i < lo || i >= hi) continue;
       const int c = j * NI + i;
-      const double d = D[c];
-      if (!(fabs(d) > 0.0)) {
+      const T d = D[c];
+      if (!(fabs(d) > T(0))) {
         pv[e] = x[c];
-        qv[e] = 0.0;
+        qv[e] = T(0);
       } else {
-        double off = 0.0;
+        T off = T(0);
         if (j > 0) {
           off += cS[c] * rowPrev[i];
         } else {
@@ -515,13 +566,13 @@ DEV void gsRow(const Instance& I, int j, const double* D, const double* cS, cons
         if (i < NI - 1) off += cE[c] * x[c + 1];
         if (j < NJ - 1) off += cN[c] * x[c + NI];
         pv[e] = (b[c] - off) / d;
-        qv[e] = (i > 0) ? -cW[c] / d : 0.0;
+        qv[e] = (i > 0) ? -cW[c] / d : T(0);
       }
       P = pv[e] + qv[e] * P;
       Q = qv[e] * Q;
     }
     blockAffineExclusiveScan(P, Q, sc);
-    double xv = P + Q * carry;  // value entering this thread's chunk
+    T xv = P + Q * carry;  // value entering this thread's chunk
 #pragma unroll
     for (int e = 0; e < 8; ++e) {
       const int i = i0 + e;
@@ -536,7 +587,7 @@ DEV void gsRow(const Instance& I, int j, const double* D, const double* cS, cons
   // next sweep) and rowPrev (the south values of row j + 1). Every read of
   // this row's old values and of rowPrev happened before the scan's barriers
   // above.
-  for (int i = threadIdx.x; i < NI; i += T) {
+  for (int i = threadIdx.x; i < NI; i += nt) {
     x[j * NI + i] = rowNew[i];
     rowPrev[i] = rowNew[i];
   }
@@ -544,15 +595,14 @@ DEV void gsRow(const Instance& I, int j, const double* D, const double* cS, cons
 
 /// `sweeps` lexicographic sweeps of one system by one CTA, row after row.
 /// Needs 2 * NI + 2 * warps doubles of shared memory.
-DEV void gsRowScanSweeps(const Instance& I, int sweeps, const double* D, const double* cS,
-                         const double* cN, const double* cW, const double* cE, const double* b,
-                         double* x, double* smem) {
-  double* rowNew = smem;        // row j, new values
-  double* rowPrev = smem + I.NI;  // row j - 1, new values
-  double* sc = smem + 2 * I.NI;
+template <typename T>
+DEV void gsRowScanSweeps(const Instance& I, int sweeps, const SysView<T>& y, T* smem) {
+  T* rowNew = smem;          // row j, new values
+  T* rowPrev = smem + I.NI;  // row j - 1, new values
+  T* sc = smem + 2 * I.NI;
   for (int sweep = 0; sweep < sweeps; ++sweep) {
     for (int j = 0; j < I.NJ; ++j) {
-      gsRow(I, j, D, cS, cN, cW, cE, b, x, rowNew, rowPrev, sc);
+      gsRow(I, j, y, rowNew, rowPrev, sc);
       __syncthreads();
     }
   }
@@ -567,28 +617,30 @@ DEV void gsRowScanSweeps(const Instance& I, int sweeps, const double* D, const d
 /// j+2, sweep s+1 row j-2). Every CTA of the cluster joins each step's
 /// barrier. Same arithmetic as gsRowScanSweeps, NJ + 2 (sweeps - 1) steps
 /// instead of sweeps * NJ.
-DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, double* smem) {
+template <typename T>
+DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, const SysView<T>& kSys,
+                            const SysView<T>& wSys, T* smem) {
   const int role = static_cast<int>(t.rank);
   const bool active = role < 2 * sweeps;
   const bool omega = active && role >= sweeps;
   const int s = active ? role % sweeps : 0;
-  const double* D = omega ? I.wD : I.kD;
-  const double* cS = omega ? I.wS : I.kS;
-  const double* cN = omega ? I.wN : I.kN;
-  const double* cW = omega ? I.wW : I.kW;
-  const double* cE = omega ? I.wE : I.kE;
-  const double* b = omega ? I.wB : I.kB;
-  double* x = omega ? I.om : I.k;
-  double* rowNew = smem;
-  double* rowPrev = smem + I.NI;
-  double* sc = smem + 2 * I.NI;
+  const SysView<T>& y = omega ? wSys : kSys;
+  T* rowNew = smem;
+  T* rowPrev = smem + I.NI;
+  T* sc = smem + 2 * I.NI;
   const int steps = I.NJ + 2 * (sweeps - 1);
   for (int step = 0; step < steps; ++step) {
     const int j = step - 2 * s;
-    if (active && j >= 0 && j < I.NJ) gsRow(I, j, D, cS, cN, cW, cE, b, x, rowNew, rowPrev, sc);
+    if (active && j >= 0 && j < I.NJ) gsRow(I, j, y, rowNew, rowPrev, sc);
     t.cl.sync();
   }
 }
+
+DEV SysView<double> kSystem(const Instance& I) { return SysView<double>{I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k}; }
+DEV SysView<double> omegaSystem(const Instance& I) {
+  return SysView<double>{I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om};
+}
+DEV SysView<float> correctionSystem(const Rows32& r) { return SysView<float>{r.D, r.S, r.N, r.W, r.E, r.r, r.x}; }
 
 // ---- phase: Rhie-Chow face fluxes (SimpleSolver.cpp:445-496) -------------------
 
@@ -926,6 +978,16 @@ DEV void phaseSstAssembly(const Instance& I, Team& t, double (&acc)[4]) {
     acc[1] += fabs(dK);
     acc[2] += fabs(bW - yw);
     acc[3] += fabs(dW);
+    if (I.precision == 1) {
+      const Rows32& a = I.tk;
+      a.D[c] = static_cast<float>(dK); a.S[c] = static_cast<float>(oK[0]);
+      a.N[c] = static_cast<float>(oK[1]); a.W[c] = static_cast<float>(oK[2]);
+      a.E[c] = static_cast<float>(oK[3]); a.r[c] = static_cast<float>(bK - yk); a.x[c] = 0.0f;
+      const Rows32& b = I.tw;
+      b.D[c] = static_cast<float>(dW); b.S[c] = static_cast<float>(oW[0]);
+      b.N[c] = static_cast<float>(oW[1]); b.W[c] = static_cast<float>(oW[2]);
+      b.E[c] = static_cast<float>(oW[3]); b.r[c] = static_cast<float>(bW - yw); b.x[c] = 0.0f;
+    }
   }
 }
 
@@ -942,8 +1004,13 @@ DEV double wallOmega(const Instance& I, double nu, double distance, double energ
 DEV void phaseSstFinish(const Instance& I, Team& t, double (&mx)[8]) {
   for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
     const int i = c % I.NI, j = c / I.NI;
-    double kc = smax(I.k[c], 0.0);
-    double wc = smax(I.om[c], kMinOmega);
+    double kRaw = I.k[c], wRaw = I.om[c];
+    if (I.precision == 1) {
+      kRaw += static_cast<double>(I.tk.x[c]);
+      wRaw += static_cast<double>(I.tw.x[c]);
+    }
+    double kc = smax(kRaw, 0.0);
+    double wc = smax(wRaw, kMinOmega);
     const uint8_t mask = I.wallMask[c];
     if (mask != 0) {
       const double d = smax(I.wallDist[c], kTinySst);
@@ -1106,6 +1173,8 @@ DEV int cgShared(const Instance& I, Team& t, Shared& sh, double* dyn, double ini
   return cgIters;
 }
 
+#include "pressure_mg.cuh"
+
 }  // namespace
 
 // ---- the kernel -----------------------------------------------------------------
@@ -1168,7 +1237,13 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
     if (stopStage == kStageMomentumAssembly) { done = it + 1; break; }
 
     // 3. Gauss-Seidel sweeps, red-black, u and v together.
-    for (int sweep = 0; sweep < I.sweeps; ++sweep) {
+    for (int sweep = 0; sweep < I.sweeps && I.precision == 1; ++sweep) {
+      for (int colour = 0; colour < 2; ++colour) {
+        gsColourMixed(I, t, colour, sweep == I.sweeps - 1 && colour == 1);
+        t.cl.sync();
+      }
+    }
+    for (int sweep = 0; sweep < I.sweeps && I.precision == 0; ++sweep) {
       for (int colour = 0; colour < 2; ++colour) {
         gsColour(I, t, colour, I.aD, I.aS, I.aN, I.aW, I.aE, I.bU, I.u, I.aD, I.aS, I.aN, I.aW,
                  I.aE, I.bV, I.v);
@@ -1218,7 +1293,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       const double initial = init[0];
       double rz = init[1];
       int cgIters = 0;
-      if (initial > 0.0 && cgInShared) {
+      if (initial > 0.0 && I.precision == 1) {
+        cgIters = pressureMixed(I, t, sh, dyn, initial);
+      } else if (initial > 0.0 && cgInShared) {
         cgIters = cgShared(I, t, sh, dyn, initial, rz);
       } else if (initial > 0.0) {
         double* dCur = I.d0;
@@ -1318,17 +1395,31 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       // state depends on the order (a colouring would move it by ~1e-3).
       if (!(flags & kFlagPlainWavefront) && I.NI <= 8 * t.T &&
           (2 * I.NI + 64) * 8 <= smemBytes) {
-        if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
-          gsRowScanPipelined(I, t, 3, dyn);
+        if (I.precision == 1) {
+          // mixed form: the same sweep map on the FP32 corrections
+          float* fs = reinterpret_cast<float*>(dyn);
+          const SysView<float> ks = correctionSystem(I.tk), ws = correctionSystem(I.tw);
+          if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
+            gsRowScanPipelined(I, t, 3, ks, ws, fs);
+          } else if (t.R == 1) {
+            gsRowScanSweeps(I, 3, ks, fs);
+            gsRowScanSweeps(I, 3, ws, fs);
+          } else if (t.rank == 0) {
+            gsRowScanSweeps(I, 3, ks, fs);
+          } else if (t.rank == 1) {
+            gsRowScanSweeps(I, 3, ws, fs);
+          }
+        } else if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
+          gsRowScanPipelined(I, t, 3, kSystem(I), omegaSystem(I), dyn);
         } else if (t.R == 1) {
           // one CTA: k, then omega
-          gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
-          gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
+          gsRowScanSweeps(I, 3, kSystem(I), dyn);
+          gsRowScanSweeps(I, 3, omegaSystem(I), dyn);
         } else if (t.rank == 0) {
           // rank 0 sweeps k, rank 1 omega
-          gsRowScanSweeps(I, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, dyn);
+          gsRowScanSweeps(I, 3, kSystem(I), dyn);
         } else if (t.rank == 1) {
-          gsRowScanSweeps(I, 3, I.wD, I.wS, I.wN, I.wW, I.wE, I.wB, I.om, dyn);
+          gsRowScanSweeps(I, 3, omegaSystem(I), dyn);
         }
       } else {
         gsWavefrontSweeps(I, t, 3, I.kD, I.kS, I.kN, I.kW, I.kE, I.kB, I.k, I.wD, I.wS, I.wN,
@@ -1430,9 +1521,9 @@ int cgSharedBytes(int NI, int NJ, int clusterSize) {
   return static_cast<int>(bytes);
 }
 
-Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
-                    int iterations, int stopStage, double tolerance, cudaStream_t stream,
-                    int smemBytes) {
+namespace {
+
+Status configureSimpleKernel() {
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -1442,6 +1533,33 @@ Status launchSimple(const Instance* dInstances, int count, int clusterSize, int 
     if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
     configured = true;
   }
+  return ok();
+}
+
+}  // namespace
+
+int maxActiveClusters(int clusterSize, int threads, int smemBytes) {
+  if (configureSimpleKernel() != CFD_OK) return 0;
+  cudaLaunchConfig_t config = {};
+  config.gridDim = dim3(static_cast<unsigned>(clusterSize * 64), 1, 1);
+  config.blockDim = dim3(static_cast<unsigned>(threads), 1, 1);
+  config.dynamicSmemBytes = static_cast<size_t>(smemBytes);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = static_cast<unsigned>(clusterSize);
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  config.attrs = attr;
+  config.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, simpleKernel, &config) != cudaSuccess) return 0;
+  return clusters;
+}
+
+Status launchSimple(const Instance* dInstances, int count, int clusterSize, int threads,
+                    int iterations, int stopStage, double tolerance, cudaStream_t stream,
+                    int smemBytes) {
+  if (Status st = configureSimpleKernel(); st != CFD_OK) return st;
   cudaLaunchConfig_t config = {};
   config.gridDim = dim3(static_cast<unsigned>(count * clusterSize), 1, 1);
   config.blockDim = dim3(static_cast<unsigned>(threads), 1, 1);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <limits>
@@ -107,7 +108,9 @@ Status Solver::create(const cfd_mesh_desc& mesh, const cfd_face_bc& bc, const Se
       s.pressureRelaxation > 1.0) {
     return fail(CFD_INVALID_ARGUMENT, "relaxation factors must lie in (0, 1]");
   }
-  if (s.precision != 0) return fail(CFD_NOT_IMPLEMENTED, "only the plain FP64 form is available in this build");
+  if (s.precision != 0 && s.precision != 1) {
+    return fail(CFD_INVALID_ARGUMENT, "precision must be 0 (plain FP64) or 1 (mixed FP32/FP64)");
+  }
   auto* solver = new Solver;
   solver->settings_ = s;
   if (Status st = solver->build(mesh, bc); st != CFD_OK) {
@@ -239,6 +242,8 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     }
   }
 
+  if (settings_.precision == 1) planMultigrid(acrossJ0);
+
   bool anchor = false;
   for (int f = 0; f < F_; ++f) {
     if (kind_[f] == CFD_BC_OUTLET || kind_[f] == CFD_BC_FARFIELD) {
@@ -326,6 +331,53 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     dWall_.outerDistance = a.take<double>(S);
     dStations_ = a.take<double>(S * kStationValues);
     dForces_ = a.take<double>(16);
+    if (!mgShape_.empty()) {
+      Multigrid& G = I.mg;
+      G.levels = static_cast<int>(mgShape_.size());
+      G.distributed = mgDistributed_;
+      G.warpFrom = G.levels;
+      for (int l = mgDistributed_; l < G.levels; ++l) {
+        if (mgShape_[l].NI * mgShape_[l].NJ <= 64) {
+          G.warpFrom = l;
+          break;
+        }
+      }
+      G.smemBytes = mgSmemBytes_;
+      // Red-black sweeps before and after the coarse correction, and on the
+      // coarsest level; CFD_MG="pre,post,coarse" overrides for tuning runs.
+      G.pre = 1;
+      G.post = 1;
+      G.coarse = 2;
+      if (const char* env = std::getenv("CFD_MG")) {
+        int a = 0, b = 0, c = 0;
+        if (std::sscanf(env, "%d,%d,%d", &a, &b, &c) == 3 && a >= 1 && b >= 1 && c >= 1 && a <= 8 &&
+            b <= 8 && c <= 64) {
+          G.pre = a;
+          G.post = b;
+          G.coarse = c;
+        }
+      }
+      for (int l = 0; l < G.levels; ++l) {
+        const MgShape& sh = mgShape_[l];
+        const std::size_t n = static_cast<std::size_t>(sh.NI) * sh.NJ;
+        MgLevel& L = G.lv[l];
+        L.NI = sh.NI;
+        L.NJ = sh.NJ;
+        L.smem = sh.smem;
+        L.D = a.take<float>(n); L.S = a.take<float>(n); L.N = a.take<float>(n);
+        L.W = a.take<float>(n); L.E = a.take<float>(n); L.inv = a.take<float>(n);
+        L.x = a.take<float>(n); L.b = a.take<float>(n);
+        L.wake = (l == 0) ? I.acrossJ0 : a.take<int>(sh.NI);
+      }
+      float** vectors[] = {&G.r, &G.q, &G.e, &G.z0, &G.z1, &G.d0, &G.d1};
+      for (float** ptr : vectors) *ptr = a.take<float>(N);
+      for (Rows32* rows : {&I.mom, &I.tk, &I.tw}) {
+        float** arrays[] = {&rows->D, &rows->S, &rows->N, &rows->W, &rows->E, &rows->r, &rows->x};
+        for (float** ptr : arrays) *ptr = a.take<float>(N);
+      }
+      I.momRv = a.take<float>(N);
+      I.momXv = a.take<float>(N);
+    }
   };
   carve(arena_);
   arenaBytes_ = arena_.bytes();
@@ -367,6 +419,10 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
   CUDA_OR_FAIL(cudaMemcpy(const_cast<int8_t*>(I.kindN), kN.data(), FN, cudaMemcpyHostToDevice));
   CUDA_OR_FAIL(cudaMemcpy(const_cast<int8_t*>(I.kindE), kE.data(), FE, cudaMemcpyHostToDevice));
   CUDA_OR_FAIL(cudaMemcpy(const_cast<int*>(I.acrossJ0), acrossJ0.data(), NI_ * sizeof(int), cudaMemcpyHostToDevice));
+  for (std::size_t l = 1; l < mgShape_.size(); ++l) {
+    CUDA_OR_FAIL(cudaMemcpy(const_cast<int*>(I.mg.lv[l].wake), mgShape_[l].wake.data(),
+                            mgShape_[l].NI * sizeof(int), cudaMemcpyHostToDevice));
+  }
   CUDA_OR_FAIL(cudaMemcpy(const_cast<double*>(I.vol), cellArea_.data(), N * sizeof(double), cudaMemcpyHostToDevice));
   CUDA_OR_FAIL(cudaMemcpy(const_cast<uint8_t*>(I.wallMask), wallMask.data(), N, cudaMemcpyHostToDevice));
   CUDA_OR_FAIL(cudaMemcpy(dCentroids_, centroid_.data(), 2 * N * sizeof(double), cudaMemcpyHostToDevice));
@@ -428,6 +484,59 @@ std::size_t Solver::estimateBytes(int NI, int NJ) {
   return (64 * N + 16 * F) * 8 + (1u << 20);
 }
 
+void Solver::planMultigrid(const std::vector<int>& wake0) {
+  mgShape_.clear();
+  mgShape_.push_back(MgShape{NI_, NJ_, -1, wake0});
+  // Halve both directions while the columns pair up and the wake map stays
+  // a map between aggregates (partner aggregates of the two cells agree).
+  while (static_cast<int>(mgShape_.size()) < kMaxMgLevels) {
+    const MgShape f = mgShape_.back();
+    if (f.NI % 2 != 0 || f.NJ < 2 || f.NI * f.NJ <= 16) break;
+    MgShape c{f.NI / 2, (f.NJ + 1) / 2, -1, std::vector<int>(f.NI / 2, -1)};
+    bool ok = true;
+    for (int I = 0; I < c.NI; ++I) {
+      const int a = f.wake[2 * I], b = f.wake[2 * I + 1];
+      const int pa = (a >= 0) ? a / 2 : -1, pb = (b >= 0) ? b / 2 : -1;
+      if (pa >= 0 && pb >= 0 && pa != pb) ok = false;
+      c.wake[I] = (pa >= 0) ? pa : pb;
+      if (c.wake[I] == I) ok = false;
+    }
+    if (!ok) break;
+    mgShape_.push_back(std::move(c));
+  }
+  const int levels = static_cast<int>(mgShape_.size());
+  mgDistributed_ = levels;
+  for (int l = 1; l < levels; ++l) {
+    if (mgShape_[l].NI * mgShape_[l].NJ <= kMgSharedCells) {
+      mgDistributed_ = l;
+      break;
+    }
+  }
+  int bytes = 0;
+  for (int l = mgDistributed_; l < levels; ++l) {
+    mgShape_[l].smem = bytes;
+    bytes += 8 * ((mgShape_[l].NI * mgShape_[l].NJ + 3) & ~3) * static_cast<int>(sizeof(float));
+  }
+  mgSmemBytes_ = bytes;
+}
+
+Status Solver::setLaunchShape(int clusterSize, int threads) {
+  if (clusterSize < 1 || clusterSize > 16 || threads < 32 || threads > 512 || threads % 32 != 0) {
+    return fail(CFD_INVALID_ARGUMENT, "cluster size must be 1..16 and threads a multiple of 32 up to 512");
+  }
+  clusterSize_ = clusterSize;
+  threads_ = threads;
+  return CFD_OK;
+}
+
+int Solver::launchSmemBytes(int clusterSize) const {
+  if (settings_.precision == 1) {
+    const int scan = (2 * NI_ + 64) * 8;  // the k/omega row sweeps
+    return std::max(mgSmemBytes_, (scan <= kMaxCgSharedBytes) ? scan : 0);
+  }
+  return cgSharedBytes(NI_, NJ_, clusterSize);
+}
+
 Solver::~Solver() {
   if (stream_ != nullptr) cudaStreamDestroy(stream_);
 }
@@ -438,6 +547,7 @@ Status Solver::uploadSettings() {
   I.NJ = NJ_;
   I.N = N_;
   I.model = model_;
+  I.precision = settings_.precision;
   I.alphaU = settings_.velocityRelaxation;
   I.alphaP = settings_.pressureRelaxation;
   I.blend = settings_.nonOrthogonalBlend;
@@ -467,7 +577,9 @@ Status Solver::setSettings(const Settings& s) {
       s.pressureRelaxation > 1.0) {
     return fail(CFD_INVALID_ARGUMENT, "relaxation factors must lie in (0, 1]");
   }
-  if (s.precision != 0) return fail(CFD_NOT_IMPLEMENTED, "only the plain FP64 form is available in this build");
+  if (s.precision != settings_.precision) {
+    return fail(CFD_INVALID_ARGUMENT, "the precision form is fixed when the solver is created");
+  }
   settings_ = s;
   return uploadSettings();
 }
@@ -673,7 +785,7 @@ Status Solver::iterate(int n, int stopStage, double tolerance, std::vector<doubl
   while (total < n) {
     const int chunk = std::min(n - total, historyCapacity_);
     if (Status st = launchSimple(dView_, 1, clusterSize_, threads_, chunk, stopStage, tolerance, stream_,
-                                 cgSharedBytes(NI_, NJ_, clusterSize_));
+                                 launchSmemBytes(clusterSize_));
         st != CFD_OK) {
       return st;
     }
@@ -1088,8 +1200,7 @@ cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out
     b->threads = solvers[k]->solver->threads();
   }
   for (cfd_handle h : b->handles) {
-    b->smemBytes = std::max(b->smemBytes, cfdb::cgSharedBytes(h->solver->cellsI(), h->solver->cellsJ(),
-                                                              b->clusterSize));
+    b->smemBytes = std::max(b->smemBytes, h->solver->launchSmemBytes(b->clusterSize));
   }
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dTable), count * sizeof(cfdb::Instance));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);

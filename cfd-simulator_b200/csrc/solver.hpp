@@ -99,6 +99,14 @@ class Solver {
   /// Rough device footprint of a solve of NI x NJ cells (the arena's layout).
   static std::size_t estimateBytes(int NI, int NJ);
   const Instance& deviceView() const { return view_; }
+  /// Dynamic shared memory a launch of this solve needs on a cluster of
+  /// `clusterSize` CTAs.
+  int launchSmemBytes(int clusterSize) const;
+  int precision() const { return settings_.precision; }
+  int wallStations() const { return wall_.count(); }
+  /// CTAs per cluster (1..16) and threads per CTA (multiple of 32, <= 512).
+  Status setLaunchShape(int clusterSize, int threads);
+  int multigridLevels() const { return static_cast<int>(mgShape_.size()); }
   cudaStream_t stream() const { return stream_; }
 
  private:
@@ -108,6 +116,9 @@ class Solver {
   Status uploadSettings();
   Status download(const double* dev, std::size_t n, double* host);
   Status upload(double* dev, const double* host, std::size_t n);
+  /// Levels of the mixed form's pressure multigrid (dimensions, wake maps,
+  /// which run on rank 0 alone from shared memory).
+  void planMultigrid(const std::vector<int>& wake0);
   /// Reference face f -> (family, index) of the device layout.
   int famOf(int f) const { return (f < jFaces_) ? 0 : 1; }
   int idxOf(int f) const;
@@ -147,7 +158,19 @@ class Solver {
   cudaStream_t stream_{nullptr};
   int clusterSize_{8};
   int threads_{512};
+
+  struct MgShape {
+    int NI, NJ, smem;
+    std::vector<int> wake;
+  };
+  std::vector<MgShape> mgShape_;
+  int mgDistributed_{0};
+  int mgSmemBytes_{0};
 };
+
+/// Levels of the multigrid with at most this many cells run on one CTA from
+/// shared memory (eight FP32 arrays per cell: ~130 KB for all of them).
+constexpr int kMgSharedCells = 3072;
 
 /// Launch the SIMPLE kernel over `count` instances (device array), one
 /// cluster of `clusterSize` CTAs each.
@@ -165,5 +188,8 @@ constexpr int kMaxCgSharedBytes = 210 * 1024;
 
 /// Cluster size used for a solve of `cells` cells (power of two, 1..16).
 int chooseClusterSize(int cells);
+
+/// Clusters of this shape the GPU holds at once (cudaOccupancyMaxActiveClusters).
+int maxActiveClusters(int clusterSize, int threads, int smemBytes);
 
 }  // namespace cfdb

@@ -287,7 +287,7 @@ typedef struct cfd_result {
   int iterations;
   int retried_cold;
   int cells;
-  int pad_;
+  int cluster_size;              /* CTAs per solve the engine ran it with */
   double continuity, momentum_x, momentum_y;
   double lift_coefficient, drag_coefficient, moment_coefficient;
   double pressure_drag_coefficient, friction_drag_coefficient;
@@ -305,6 +305,12 @@ cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* request, int* id);
 cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued);
 /* Move up to `capacity` finished results into `out`; *count gets how many. */
 cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* count);
+/* Pressure coefficient at every wall station of a finished solve (upper
+ * surface from the leading edge, then the lower), as cfd_gpu_forces returns
+ * it (post::extractSurface, SurfaceData.cpp:101-348). cp = NULL only stores
+ * the station count; otherwise capacity must hold it, and the data are
+ * released after the copy. Diverged solves have none. */
+cfd_status cfd_engine_surface(cfd_engine e, int id, double* cp, int capacity, int* stations);
 /* Seconds on the engine clock (for submit-time bookkeeping by callers). */
 double cfd_engine_clock(cfd_engine e);
 cfd_status cfd_engine_destroy(cfd_engine e);

@@ -43,9 +43,9 @@ class Case:
         self.packed = g["settings"]
         self.initial = (g["u0"], g["v0"], g["p0"], g["rho0"], g["mu0"])
 
-    def settings(self) -> cb.Settings:
+    def settings(self, precision: int = 0) -> cb.Settings:
         p = self.packed
-        return cb.Settings.defaults(
+        return cb.Settings.defaults(precision=precision,
             velocity_relaxation=p[0], pressure_relaxation=p[1], momentum_sweeps=int(p[2]),
             pressure_iterations=int(p[3]), pressure_tolerance=p[4], scheme=int(p[5]),
             turbulence_relaxation=p[6], inflow_intensity=p[7], inflow_viscosity_ratio=p[8],
@@ -57,8 +57,8 @@ class Case:
         s.initialise(*self.initial)
         return s
 
-    def device(self) -> "cb.SimpleSolver":
-        s = cb.SimpleSolver.create(self.mesh, self.conditions, self.settings())
+    def device(self, precision: int = 0) -> "cb.SimpleSolver":
+        s = cb.SimpleSolver.create(self.mesh, self.conditions, self.settings(precision))
         s.set_turbulence_model(self.model)
         s.initialise(*self.initial)
         return s

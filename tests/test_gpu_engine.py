@@ -2,6 +2,8 @@
 a mix are the same, results equal a direct solve, admission respects the
 memory budget, and a diverging solve is retried cold once (Polar.cpp:109-121)
 and then reported diverged."""
+import os
+
 import numpy as np
 import pytest
 
@@ -41,18 +43,32 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
             assert x == pytest.approx(y, rel=1e-12, abs=1e-15)
 
 
-def test_engine_result_equals_a_direct_solve():
-    req = _req(alpha=4.0)
-    res = cb.Engine(chunk=32).run([req])[0]
+@pytest.mark.parametrize("precision", [0, 1])
+def test_engine_result_equals_a_direct_solve(precision):
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=10.0, precision=precision)
+    req = cb.request("0012", 4.0, 1e6, tolerance=1e-8, max_iterations=3000, settings=settings, **TINY)
+    engine = cb.Engine(chunk=32)
+    res = engine.run([req])[0]
+    cp_engine = engine.surface(res.id)
     mesh = cb.cgrid("0012", upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0,
                     **TINY)
-    s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0),
-                               cb.Settings.defaults(inflow_viscosity_ratio=10.0))
+    # the same launch shape as the engine's tuner chose (the reduction order
+    # depends on the CTAs per solve)
+    old = os.environ.get("CFD_CLUSTER_SIZE")
+    os.environ["CFD_CLUSTER_SIZE"] = str(res.cluster_size)
+    try:
+        s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0), settings)
+    finally:
+        if old is None:
+            os.environ.pop("CFD_CLUSTER_SIZE")
+        else:
+            os.environ["CFD_CLUSTER_SIZE"] = old
     s.set_turbulence_model(cb.MODEL_SST)
     s.initialise(*cb.uniform_field(mesh, 1.0, 4.0, 1.0, 1e6))
     taken, mon = s.converge(3000, 1e-8)
-    f, _, _ = s.forces(1.0, 4.0, 1.0)
+    f, cp, _ = s.forces(1.0, 4.0, 1.0)
     assert res.status == 0 and res.iterations == taken
+    assert np.array_equal(cp_engine, cp)
     assert res.lift_coefficient == pytest.approx(f.lift_coefficient, rel=1e-12)
     assert res.drag_coefficient == pytest.approx(f.drag_coefficient, rel=1e-12)
     assert res.continuity == pytest.approx(mon.continuity, rel=1e-12)
@@ -89,3 +105,10 @@ def test_a_diverging_solve_is_retried_cold_once_then_reported():
 def test_iteration_limit_is_reported():
     r = cb.Engine(chunk=16).run([_req(tol=1e-30, cap=40)])[0]
     assert r.status == 1 and r.iterations == 40
+
+
+def test_tuned_shape_is_fixed_per_grid_and_reported():
+    reqs = [_req(alpha=a, tol=1e-5, cap=200) for a in (0.0, 2.0)]
+    res = cb.Engine(chunk=32).run(reqs)
+    shapes = {r.cluster_size for r in res}
+    assert len(shapes) == 1 and shapes.pop() in (4, 6, 8, 16)
