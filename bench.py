@@ -120,9 +120,10 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workload ---
 
-def build_solvers(cb):
+def build_solvers(cb, precision: int = 0):
     mesh = cb.cgrid(WORKLOAD["designation"], **{k: v for k, v in WORKLOAD.items() if k != "designation"})
-    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO)
+    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
+                                    precision=precision)
     solvers = []
     for alpha in ALPHAS:
         s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
@@ -130,6 +131,41 @@ def build_solvers(cb):
         s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, REYNOLDS))
         solvers.append(s)
     return mesh, solvers
+
+
+def converge_both_forms(cb, tolerance: float = 1e-6, cap: int = 6000) -> dict:
+    """The benchmark pair solved to convergence in each form from the uniform
+    start, batched (both solves in one launch per chunk, each stopping on its
+    own): solves/min, iterations, and the mixed answers' differences from
+    the FP64 ones (Cl, Cd, Cm, and Cp at every station)."""
+    import torch
+    out = {"tolerance": tolerance, "cap": cap}
+    answers = {}
+    for name, precision in (("plain", 0), ("mixed", 1)):
+        mesh, solvers = build_solvers(cb, precision)
+        batch = cb.Batch(solvers)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        taken, _ = batch.iterate(cap, tolerance)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        forces = [s.forces(1.0, a, 1.0) for s, a in zip(solvers, ALPHAS)]
+        answers[name] = forces
+        out[name] = {"solves_per_min": 60.0 * len(solvers) / wall, "wall_s": wall,
+                     "iterations": list(taken),
+                     "cl": [f[0].lift_coefficient for f in forces],
+                     "cd": [f[0].drag_coefficient for f in forces]}
+        batch.close()
+        for s in solvers:
+            s.close()
+    p, m = answers["plain"], answers["mixed"]
+    out["mixed_vs_plain"] = {
+        "solves_per_min_ratio": out["mixed"]["solves_per_min"] / out["plain"]["solves_per_min"],
+        "dcl": [abs(b[0].lift_coefficient - a[0].lift_coefficient) for a, b in zip(p, m)],
+        "dcd": [abs(b[0].drag_coefficient - a[0].drag_coefficient) for a, b in zip(p, m)],
+        "dcm": [abs(b[0].moment_coefficient - a[0].moment_coefficient) for a, b in zip(p, m)],
+        "dcp_inf": [float(np.max(np.abs(b[1] - a[1]))) for a, b in zip(p, m)]}
+    return out
 
 
 def measured_peak() -> tuple[float, str]:
@@ -363,6 +399,8 @@ def run_ours(args) -> None:
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
+        if world == 1 and not args.no_convergence:
+            line["convergence"] = converge_both_forms(cb)
         print(json.dumps(line), flush=True)
     batch.close()
     for s in solvers:
@@ -526,6 +564,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-convergence", action="store_true",
+                    help="skip solving the pair to convergence in both forms")
     ap.add_argument("--workload", choices=("c2", "polar", "serve"), default="c2",
                     help="c2: the benchmark line (default); polar / serve: engine workloads")
     ap.add_argument("--tolerance", type=float, default=1e-6)

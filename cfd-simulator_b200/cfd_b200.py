@@ -92,7 +92,7 @@ class Settings(C.Structure):
                 ("turbulence_relaxation", C.c_double), ("inflow_intensity", C.c_double),
                 ("inflow_viscosity_ratio", C.c_double), ("inflow_length_scale", C.c_double),
                 ("non_orthogonal_correctors", C.c_int), ("non_orthogonal_blend", C.c_double),
-                ("precision", C.c_int)]
+                ("precision", C.c_int), ("inner_iterations", C.c_int)]
 
     @staticmethod
     def defaults(**overrides) -> "Settings":

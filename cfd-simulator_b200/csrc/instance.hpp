@@ -102,6 +102,7 @@ struct Instance {
   int NI, NJ, N;
   int model;  // 0 none, 1 laminar closure, 2 k-omega SST
   int precision;  // 0 plain FP64, 1 mixed FP32/FP64
+  int mgCap;      // mixed form: multigrid-CG iterations per pressure correction
 
   // ---- settings (SimpleSettings) ----
   double alphaU, alphaP, blend, alphaT;

@@ -5,8 +5,8 @@
 // and, at its cap of 200 iterations, reduces the L1 residual of the p'
 // system by only ~2.5x on a 384x96 C-grid (it would need ~1000 iterations
 // for the reference's 1% target). The mixed form solves the same system to
-// the same stopping rule (sum |r| <= tol * sum |r0|, at most `cgMax`
-// iterations) with a stronger inner solver:
+// the same stopping rule (sum |r| <= tol * sum |r0|) with a stronger inner
+// solver, at most `mgCap` iterations (the settings' inner_iterations):
 //
 //   outer (FP64):  x = 0, r = b;  repeat: inner solve A e = r in FP32,
 //                  x += e, r = b - A x (FP64 rows), stop on the L1 rule.
@@ -57,9 +57,9 @@ DEV Lv sharedLevel(const MgLevel& M, char* smem) {
   return Lv{M.NI, M.NJ, p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, p + 6 * n, p + 7 * n, M.wake};
 }
 
-DEV Lv levelView(const Instance& I, int l, char* smem) {
-  const MgLevel& M = I.mg.lv[l];
-  return (l < I.mg.distributed) ? globalLevel(M) : sharedLevel(M, smem);
+DEV Lv levelView(const Multigrid& G, int l, char* smem) {
+  const MgLevel& M = G.lv[l];
+  return (l < G.distributed) ? globalLevel(M) : sharedLevel(M, smem);
 }
 
 DEV Span bandOf(const Lv& L, const Team& t) {
@@ -132,45 +132,33 @@ DEV float offSumProlonged(const Lv& L, const float* ec, int NIc, int c, int i, i
   return s;
 }
 
-/// Gauss-Seidel half sweep over the cells of one colour. Each thread takes
-/// up to four cells at a time and loads everything for them before it
-/// stores, so the loads of the four overlap (a store to x could otherwise
-/// alias the next cell's loads and serialise them).
+/// Gauss-Seidel half sweep over the cells of one colour. The new values are
+/// written through a pointer declared not to alias the one the neighbours
+/// are read through (they never touch the same cells: a colour's neighbours
+/// are all of the other colour), so consecutive cells' loads can overlap.
 template <bool kProlonged>
 DEV void sweepCells(const Lv& L, const Span& s, int colour, const float* ec, int NIc) {
+  float* __restrict__ xw = L.x;
   const int rows = s.j1 - s.j0;
   if ((L.NI & 1) != 0) {
     // the coarsest level may have an odd width: plain loop
     forCells(L, s, [&](int c, int i, int j) {
       if (((i + j) & 1) != colour) return;
       const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
-      L.x[c] = (L.b[c] - off) * L.inv[c];
+      xw[c] = (L.b[c] - off) * L.inv[c];
     });
     return;
   }
   const int half = L.NI >> 1;
   const int count = rows * half;
-  for (int m0 = s.tid; m0 < count; m0 += 4 * s.T) {
-    float val[4];
-    int at[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int m = m0 + k * s.T;
-      at[k] = -1;
-      if (m < count) {
-        const int jj = m / half;
-        const int j = s.j0 + jj;
-        const int i = 2 * (m - jj * half) + ((colour + j) & 1);
-        const int c = j * L.NI + i;
-        const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
-        val[k] = (L.b[c] - off) * L.inv[c];
-        at[k] = c;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (at[k] >= 0) L.x[at[k]] = val[k];
-    }
+#pragma unroll 2
+  for (int m = s.tid; m < count; m += s.T) {
+    const int jj = m / half;
+    const int j = s.j0 + jj;
+    const int i = 2 * (m - jj * half) + ((colour + j) & 1);
+    const int c = j * L.NI + i;
+    const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
+    xw[c] = (L.b[c] - off) * L.inv[c];
   }
 }
 
@@ -199,31 +187,20 @@ DEV float aggregateResidual(const Lv& F, int I, int J) {
 
 /// Restrict the fine residual b - A x to the coarse right-hand side (sum over
 /// each aggregate). With `start`, also begin the coarse level: red cells
-/// b / D, black 0. Four coarse cells per thread at a time, loads first.
+/// b / D, black 0.
 template <bool kStart>
 DEV void restrictCells(const Lv& F, const Lv& C, const Span& s) {
+  float* __restrict__ bw = C.b;
+  float* __restrict__ xw = C.x;
   const int count = (s.j1 - s.j0) * C.NI;
-  for (int m0 = s.tid; m0 < count; m0 += 4 * s.T) {
-    float val[4];
-    int at[4], colour[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int m = m0 + k * s.T;
-      at[k] = -1;
-      if (m < count) {
-        const int jj = m / C.NI;
-        const int I = m - jj * C.NI, J = s.j0 + jj;
-        val[k] = aggregateResidual(F, I, J);
-        at[k] = J * C.NI + I;
-        colour[k] = (I + J) & 1;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      if (at[k] < 0) continue;
-      C.b[at[k]] = val[k];
-      if (kStart) C.x[at[k]] = (colour[k] == 0) ? val[k] * C.inv[at[k]] : 0.0f;
-    }
+#pragma unroll 2
+  for (int m = s.tid; m < count; m += s.T) {
+    const int jj = m / C.NI;
+    const int I = m - jj * C.NI, J = s.j0 + jj;
+    const int cc = J * C.NI + I;
+    const float val = aggregateResidual(F, I, J);
+    bw[cc] = val;
+    if (kStart) xw[cc] = (((I + J) & 1) == 0) ? val * C.inv[cc] : 0.0f;
   }
 }
 
@@ -268,8 +245,7 @@ DEV void galerkin(const Lv& F, const Lv& C, const Span& s) {
 /// entry level `first` holds its right-hand side and its red start; on exit
 /// its x is final.
 template <typename Sync, typename SpanOf>
-DEV void localCycle(const Instance& I, char* smem, int first, Sync sync, SpanOf spanOf) {
-  const Multigrid& G = I.mg;
+DEV void localCycle(const Multigrid& G, char* smem, int first, Sync sync, SpanOf spanOf) {
   const int L = G.levels;
   int l = first;
   for (; l < L; ++l) {
@@ -307,8 +283,7 @@ DEV void localCycle(const Instance& I, char* smem, int first, Sync sync, SpanOf 
 /// cluster restricted it into global memory), run the V-cycle below it
 /// (levels of at most 64 cells on warp 0 alone), and publish that level's x
 /// to global memory for the cluster's prolongation.
-DEV void sharedCycle(const Instance& I, char* smem) {
-  const Multigrid& G = I.mg;
+DEV void sharedCycle(const Multigrid& G, char* smem) {
   const int L = G.levels, m = G.distributed, w = G.warpFrom;
   {
     // the cluster restricted into level m's global right-hand side
@@ -325,7 +300,7 @@ DEV void sharedCycle(const Instance& I, char* smem) {
   if (w == m) {
     // every shared level is small: warp 0 runs them all
     __syncthreads();
-    if (threadIdx.x < 32) localCycle(I, smem, m, warp, [](const Lv& A) { return warpOf(A); });
+    if (threadIdx.x < 32) localCycle(G, smem, m, warp, [](const Lv& A) { return warpOf(A); });
   } else {
     // block levels [m, w), then warp levels [w, L)
     int l = m;
@@ -349,7 +324,7 @@ DEV void sharedCycle(const Instance& I, char* smem) {
     }
     if (w < L) {
       __syncthreads();
-      if (threadIdx.x < 32) localCycle(I, smem, w, warp, [](const Lv& A) { return warpOf(A); });
+      if (threadIdx.x < 32) localCycle(G, smem, w, warp, [](const Lv& A) { return warpOf(A); });
     }
     for (l = ((w < L) ? w : L - 1) - 1; l >= m; --l) {
       const Lv A = sharedLevel(G.lv[l], smem);
@@ -374,11 +349,10 @@ DEV void sharedCycle(const Instance& I, char* smem) {
 /// barrier). On exit, after a cluster barrier, z is complete except for the
 /// last red half sweep on the fine level, which the caller fuses with its
 /// reduction.
-DEV void vcycle(const Instance& I, Team& t, char* smem, float* z) {
-  const Multigrid& G = I.mg;
+DEV void vcycle(const Multigrid& G, Team& t, char* smem, float* z) {
   const int L = G.levels, Ld = G.distributed;
   auto view = [&](int l) {
-    Lv v = levelView(I, l, smem);
+    Lv v = levelView(G, l, smem);
     if (l == 0) {
       v.x = z;
       v.b = G.r;
@@ -409,7 +383,7 @@ DEV void vcycle(const Instance& I, Team& t, char* smem, float* z) {
       const Lv C = globalLevel(G.lv[l + 1]);
       restrictCells<false>(F, C, bandOf(C, t));
       t.cl.sync();
-      if (t.rank == 0) sharedCycle(I, smem);
+      if (t.rank == 0) sharedCycle(G, smem);
     }
   }
   for (int l = (Ld < L) ? Ld - 1 : L - 2; l >= 0; --l) {
@@ -433,7 +407,15 @@ DEV void vcycle(const Instance& I, Team& t, char* smem, float* z) {
 /// the inner iterations run (the monitor's pressure iterations).
 __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh, double* dyn,
                                           double initial) {
-  const Multigrid& G = I.mg;
+  // The multigrid descriptor is read at every phase: keep a copy on chip.
+  __shared__ Multigrid mgs;
+  {
+    const int* src = reinterpret_cast<const int*>(&I.mg);
+    int* dst = reinterpret_cast<int*>(&mgs);
+    for (int k = t.tid; k < static_cast<int>(sizeof(Multigrid) / sizeof(int)); k += t.T) dst[k] = src[k];
+    __syncthreads();
+  }
+  const Multigrid& G = mgs;
   char* smem = reinterpret_cast<char*>(dyn);
   const int NI = I.NI, NJ = I.NJ;
   const int op1[1] = {kSum};
@@ -452,15 +434,15 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
   }
   for (int l = 1; l < G.distributed; ++l) {
     t.cl.sync();
-    const Lv C = levelView(I, l, smem);
-    galerkin(levelView(I, l - 1, smem), C, bandOf(C, t));
+    const Lv C = levelView(G, l, smem);
+    galerkin(levelView(G, l - 1, smem), C, bandOf(C, t));
   }
   t.cl.sync();
   if (G.distributed < G.levels && t.rank == 0) {
     for (int l = G.distributed; l < G.levels; ++l) {
       if (l > G.distributed) __syncthreads();
       const Lv C = sharedLevel(G.lv[l], smem);
-      galerkin(levelView(I, l - 1, smem), C, wholeOf(C));
+      galerkin(levelView(G, l - 1, smem), C, wholeOf(C));
     }
     // the first V-cycle's barriers order these rows before their use
   }
@@ -470,7 +452,7 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
   float* q = G.q;
   float* e = G.e;
   int total = 0;
-  for (int refine = 0; refine < 3 && total < I.cgMax; ++refine) {
+  for (int refine = 0; refine < 3 && total < I.mgCap; ++refine) {
     // ---- inner solve of A e = r in FP32 ----
     float* zc = G.z0;
     float* zp = G.z1;
@@ -483,7 +465,7 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
       e[c] = 0.0f;
       zc[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
     }
-    vcycle(I, t, smem, zc);
+    vcycle(G, t, smem, zc);
     double rz;
     {
       Lv Z = F0;
@@ -499,15 +481,21 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
       rz = v1[0];
     }
     double beta = 0.0;
-    for (int it = 0; total < I.cgMax; ++it) {
+    for (int it = 0; total < I.mgCap; ++it) {
       // q = A d' with d' = z + beta d, formed for each cell and its neighbours.
       double dq[1] = {0.0};
       const float fb = static_cast<float>(beta);
+      {
+      const float* __restrict__ zR = zc;
+      const float* __restrict__ dR = dc;
+      float* __restrict__ dW = dn;
+      float* __restrict__ qW = q;
+#pragma unroll 2
       for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        const int i = c % NI, j = c / NI;
-        auto dir = [&](int n) { return (it == 0) ? zc[n] : zc[n] + fb * dc[n]; };
+        const int j = c / NI, i = c - j * NI;
+        auto dir = [&](int n) { return (it == 0) ? zR[n] : zR[n] + fb * dR[n]; };
         const float dv = dir(c);
-        dn[c] = dv;
+        dW[c] = dv;
         float y = F0.D[c] * dv;
         if (j > 0) {
           y += F0.S[c] * dir(c - NI);
@@ -518,8 +506,9 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
         if (j < NJ - 1) y += F0.N[c] * dir(c + NI);
         if (i > 0) y += F0.W[c] * dir(c - 1);
         if (i < NI - 1) y += F0.E[c] * dir(c + 1);
-        q[c] = y;
+        qW[c] = y;
         dq[0] += static_cast<double>(dv) * static_cast<double>(y);
+      }
       }
       {
         float* tmp = dc;
@@ -530,25 +519,41 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
       if (!(fabs(dq[0]) > 0.0) || !isfinite(dq[0])) break;
       const float alpha = static_cast<float>(rz / dq[0]);
       double v3[3] = {0.0, 0.0, 0.0};
+      {
+      float* __restrict__ eW = e;
+      float* __restrict__ rW = r;
+      float* __restrict__ zW = zp;
+      const float* __restrict__ dR = dc;
+      const float* __restrict__ qR = q;
+#pragma unroll 2
       for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        const int i = c % NI, j = c / NI;
-        e[c] += alpha * dc[c];
-        const float rc = r[c] - alpha * q[c];
-        r[c] = rc;
+        const int j = c / NI, i = c - j * NI;
+        eW[c] += alpha * dR[c];
+        const float rc = rW[c] - alpha * qR[c];
+        rW[c] = rc;
         v3[2] += fabs(static_cast<double>(rc));
-        zp[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
+        zW[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
+      }
       }
       ++total;
-      vcycle(I, t, smem, zp);
+      vcycle(G, t, smem, zp);
       {
         Lv Z = F0;
         Z.x = zp;
         Z.b = r;
+        float* __restrict__ zW = zp;
+#pragma unroll 2
         for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-          const int i = c % NI, j = c / NI;
-          if (((i + j) & 1) == 0) zp[c] = (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c];
+          const int j = c / NI, i = c - j * NI;
+          float zv;
+          if (((i + j) & 1) == 0) {
+            zv = (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c];
+            zW[c] = zv;
+          } else {
+            zv = zp[c];
+          }
           const double rc = static_cast<double>(r[c]);
-          v3[0] += rc * static_cast<double>(zp[c]);
+          v3[0] += rc * static_cast<double>(zv);
           v3[1] += rc * static_cast<double>(zc[c]);
         }
       }

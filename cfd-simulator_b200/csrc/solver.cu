@@ -56,6 +56,7 @@ Settings fromC(const cfd_settings& s) {
   o.nonOrthogonalCorrectors = s.non_orthogonal_correctors;
   o.nonOrthogonalBlend = s.non_orthogonal_blend;
   o.precision = s.precision;
+  o.innerIterations = s.inner_iterations;
   return o;
 }
 
@@ -73,6 +74,7 @@ void toC(const Settings& s, cfd_settings* o) {
   o->non_orthogonal_correctors = s.nonOrthogonalCorrectors;
   o->non_orthogonal_blend = s.nonOrthogonalBlend;
   o->precision = s.precision;
+  o->inner_iterations = s.innerIterations;
 }
 
 // ---- device arena ---------------------------------------------------------------
@@ -111,6 +113,7 @@ Status Solver::create(const cfd_mesh_desc& mesh, const cfd_face_bc& bc, const Se
   if (s.precision != 0 && s.precision != 1) {
     return fail(CFD_INVALID_ARGUMENT, "precision must be 0 (plain FP64) or 1 (mixed FP32/FP64)");
   }
+  if (s.innerIterations < 0) return fail(CFD_INVALID_ARGUMENT, "inner_iterations must be >= 0");
   auto* solver = new Solver;
   solver->settings_ = s;
   if (Status st = solver->build(mesh, bc); st != CFD_OK) {
@@ -548,6 +551,8 @@ Status Solver::uploadSettings() {
   I.N = N_;
   I.model = model_;
   I.precision = settings_.precision;
+  I.mgCap = (settings_.innerIterations > 0) ? std::min(settings_.innerIterations, settings_.pressureIterations)
+                                            : settings_.pressureIterations;
   I.alphaU = settings_.velocityRelaxation;
   I.alphaP = settings_.pressureRelaxation;
   I.blend = settings_.nonOrthogonalBlend;

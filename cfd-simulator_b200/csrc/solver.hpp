@@ -57,6 +57,7 @@ struct Settings {
   int nonOrthogonalCorrectors{1};
   double nonOrthogonalBlend{1.0};
   int precision{0};
+  int innerIterations{16};
 };
 
 Settings fromC(const cfd_settings& s);

@@ -87,6 +87,8 @@ typedef struct cfd_settings {
   int non_orthogonal_correctors;   /* 1 */
   double non_orthogonal_blend;     /* 1.0 */
   int precision;                   /* 0 plain FP64 (the drop-in), 1 mixed FP32/FP64 */
+  int inner_iterations;            /* mixed form: cap on the multigrid-CG iterations of one
+                                      pressure correction (0: pressure_iterations); 16 */
 } cfd_settings;
 
 /* solver::SolverMonitor (SimpleSolver.hpp:135-154), flattened; plus the

@@ -35,8 +35,13 @@ def _l1_residual(c, d):
 @pytest.mark.parametrize("warm", [0, 5])
 @pytest.mark.parametrize("name", CASES)
 def test_pressure_solve_meets_the_reference_stopping_rule(name, warm):
+    # inner_iterations = 0: the multigrid CG may take up to pressure_iterations
     c = Case(name)
-    d = c.device(precision=1)
+    s = c.settings(precision=1)
+    s.inner_iterations = 0
+    d = cb.SimpleSolver.create(c.mesh, c.conditions, s)
+    d.set_turbulence_model(c.model)
+    d.initialise(*c.initial)
     if warm:
         d.iterate(warm)
     mon = d.iterate_partial("PRESSURE_SOLVE")
@@ -99,6 +104,17 @@ def test_converged_mixed_solve_reaches_the_reference_fixed_point(name):
     assert f.drag_coefficient == pytest.approx(ref[1], rel=1e-6)
     assert f.moment_coefficient == pytest.approx(ref[2], rel=1e-6, abs=1e-9)
     assert np.max(np.abs(cp - g["converged/cp"])) < 1e-6
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_default_inner_cap_bounds_the_pressure_solve(name):
+    c = Case(name)
+    d = c.device(precision=1)
+    d.iterate(5)
+    mon = d.iterate_partial("PRESSURE_SOLVE")
+    res, b = _l1_residual(c, d)
+    assert 0 < mon.pressure_iterations <= cb.Settings.defaults().inner_iterations
+    assert res < 0.5 * b
 
 
 def test_precision_is_fixed_at_create():
