@@ -361,14 +361,8 @@ def run_ours(args) -> None:
     e2e_s = time.perf_counter() - t0
 
     # multi-rank: max time over ranks, cells summed
-    totals = np.array([total_s, e2e_s, cells], dtype=np.float64)
     if dist is not None:
-        t = torch.tensor(totals[:2], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        c = torch.tensor([cells], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        total_s, e2e_s = (float(x) for x in t.tolist())
-        all_cells = float(c.item())
+        (total_s, e2e_s), all_cells = reduce_over_ranks([total_s, e2e_s], cells, dist, "cuda")
     else:
         all_cells = float(cells)
     value = all_cells * args.steps / total_s
@@ -408,6 +402,17 @@ def run_ours(args) -> None:
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def reduce_over_ranks(times, cells, dist, device):
+    """Replicas: the job's times are the slowest rank's, its work the sum of
+    every rank's. Every rank calls this with the same number of values."""
+    import torch
+    t = torch.tensor([float(x) for x in times], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return [float(x) for x in t.tolist()], float(c.item())
 
 
 # ------------------------------------------------- engine workloads ---
@@ -479,7 +484,8 @@ def run_polar(args) -> None:
         summary = _summarise(results, wall, cb)
         summary["polar"] = [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
                              "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
-                             "iterations": r.iterations, "cl": r.lift_coefficient,
+                             "iterations": r.iterations, "ctas": r.cluster_size,
+                             "cl": r.lift_coefficient,
                              "cd": r.drag_coefficient, "cm": r.moment_coefficient,
                              "continuity": r.continuity} for r in results]
         out[form] = summary

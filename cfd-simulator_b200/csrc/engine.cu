@@ -24,6 +24,7 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -68,6 +69,12 @@ MeshKey keyOf(const cfd_request& r) {
           r.grid_vertical_chords};
 }
 
+/// Tuned launch shapes per (cells I, cells J, model, precision), shared by
+/// every engine of the process, so a grid runs with one shape (and one
+/// reduction order) whichever engine it is submitted to.
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_shapes;
+std::mutex g_shapesMutex;
+
 }  // namespace
 
 struct Engine {
@@ -80,7 +87,6 @@ struct Engine {
   std::vector<cfd_result> done;
   std::map<int, std::vector<double>> surfaces;  // Cp per wall station of each finished solve
   std::map<MeshKey, std::shared_ptr<const HostMesh>> meshes;
-  std::map<std::tuple<int, int, int, int>, std::pair<int, int>> shapes;  // tuned launch shapes
   std::chrono::steady_clock::time_point t0{std::chrono::steady_clock::now()};
   // device status area: per slot, chunk monitors then the iteration count
   double* dStatus{nullptr};
@@ -153,48 +159,78 @@ struct Engine {
     return ok();
   }
 
-  /// The launch shape of a grid: among clusters of 4, 6, 8 and 16 CTAs of 512
+  /// The launch shape of a grid: among clusters of 4, 8 and 16 CTAs of 512
   /// threads, the one that gives the most solve-iterations per second on a
-  /// full GPU, (clusters resident at once) / (time per iteration), timed on
-  /// a scratch solve of the same grid, model and precision from its uniform
-  /// start. Chosen once per (cells I, cells J, model, precision) and cached,
-  /// so a request runs with the same shape, and gives the same bits, whatever
-  /// else is in the engine. CFD_ENGINE_TUNE=0 keeps the solver's default.
+  /// full GPU. Each candidate is timed the way the engine runs it when busy:
+  /// as many scratch solves of the grid (same model and precision, from their
+  /// uniform start) as the GPU holds at once for that shape
+  /// (cudaOccupancyMaxActiveClusters), in one launch over a descriptor table,
+  /// so the shared L2 and HBM traffic of that many resident solves is in the
+  /// measurement. Chosen once per (cells I, cells J, model, precision) and
+  /// kept for the process, so a request runs with the same shape, and gives
+  /// the same bits, whatever else is in the engine. CFD_ENGINE_TUNE=0 keeps the solver's
+  /// default shape.
   Status tunedShape(const Pending& q, const Solver& s, std::pair<int, int>* out) {
     const auto key = std::make_tuple(s.cellsI(), s.cellsJ(), q.request.model, s.precision());
-    if (auto it = shapes.find(key); it != shapes.end()) {
+    std::lock_guard<std::mutex> lock(g_shapesMutex);
+    if (auto it = g_shapes.find(key); it != g_shapes.end()) {
       *out = it->second;
       return ok();
     }
     std::pair<int, int> best{s.clusterSize(), s.threads()};
     const char* env = std::getenv("CFD_ENGINE_TUNE");
     if (env == nullptr || std::atoi(env) != 0) {
-      std::unique_ptr<Solver> probe;
-      if (Status st = makeSolver(q, &probe); st != CFD_OK) return st;
-      double bestScore = -1.0;
-      for (int R : {4, 6, 8, 16}) {
+      const int T = 512;
+      std::vector<std::pair<int, int>> candidates;  // (R, resident clusters)
+      int most = 0;
+      for (int R : {4, 8, 16}) {
         if (R > s.cellsJ()) continue;
-        const int T = 512;
-        if (probe->setLaunchShape(R, T) != CFD_OK) continue;
-        const int resident = maxActiveClusters(R, T, probe->launchSmemBytes(R));
+        const int resident = maxActiveClusters(R, T, s.launchSmemBytes(R));
         if (resident <= 0) continue;
-        std::vector<double> u, v, p, rho, mu;
-        uniform(q.request, probe->cells(), &u, &v, &p, &rho, &mu);
-        if (probe->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()) != CFD_OK) continue;
-        int taken = 0;
-        if (probe->iterate(3, kStageEnd, -1.0, nullptr, &taken) != CFD_OK) continue;
-        const auto t0 = std::chrono::steady_clock::now();
-        if (probe->iterate(8, kStageEnd, -1.0, nullptr, &taken) != CFD_OK) continue;
-        const double perIteration =
-            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / 8.0;
-        const double score = resident / perIteration;
-        if (score > bestScore) {
-          bestScore = score;
-          best = {R, T};
+        candidates.emplace_back(R, resident);
+        most = std::max(most, resident);
+      }
+      // scratch solves, within a quarter of the engine's memory budget
+      const std::size_t each = std::max<std::size_t>(s.deviceBytes(), 1);
+      const int affordable = static_cast<int>(std::max<std::size_t>(1, budget / 4 / each));
+      const int copies = std::min({most, affordable, 40});
+      std::vector<std::unique_ptr<Solver>> probes;
+      for (int k = 0; k < copies; ++k) {
+        std::unique_ptr<Solver> p;
+        if (makeSolver(q, &p) != CFD_OK) break;
+        probes.push_back(std::move(p));
+      }
+      Instance* table = nullptr;
+      if (!probes.empty() &&
+          cudaMalloc(reinterpret_cast<void**>(&table), probes.size() * sizeof(Instance)) == cudaSuccess) {
+        std::vector<Instance> rows;
+        for (const auto& p : probes) rows.push_back(p->deviceView());
+        double bestScore = -1.0;
+        if (cudaMemcpy(table, rows.data(), rows.size() * sizeof(Instance), cudaMemcpyHostToDevice) ==
+            cudaSuccess) {
+          for (const auto& [R, resident] : candidates) {
+            const int n = std::min<int>(resident, static_cast<int>(probes.size()));
+            const int smem = probes[0]->launchSmemBytes(R);
+            if (launchSimple(table, n, R, T, 2, kStageEnd, -1.0, nullptr, smem) != CFD_OK) continue;
+            if (cudaDeviceSynchronize() != cudaSuccess) break;
+            const auto t0 = std::chrono::steady_clock::now();
+            if (launchSimple(table, n, R, T, 6, kStageEnd, -1.0, nullptr, smem) != CFD_OK) continue;
+            if (cudaDeviceSynchronize() != cudaSuccess) break;
+            const double perIteration =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() / 6.0;
+            // n solves advance one iteration per perIteration; a full GPU
+            // holds `resident` of them (n < resident only when memory is short)
+            const double score = n / perIteration * (static_cast<double>(resident) / n);
+            if (score > bestScore) {
+              bestScore = score;
+              best = {R, T};
+            }
+          }
         }
+        cudaFree(table);
       }
     }
-    shapes[key] = best;
+    g_shapes[key] = best;
     *out = best;
     return ok();
   }

@@ -138,27 +138,44 @@ DEV float offSumProlonged(const Lv& L, const float* ec, int NIc, int c, int i, i
 /// are all of the other colour), so consecutive cells' loads can overlap.
 template <bool kProlonged>
 DEV void sweepCells(const Lv& L, const Span& s, int colour, const float* ec, int NIc) {
-  float* __restrict__ xw = L.x;
   const int rows = s.j1 - s.j0;
   if ((L.NI & 1) != 0) {
     // the coarsest level may have an odd width: plain loop
     forCells(L, s, [&](int c, int i, int j) {
       if (((i + j) & 1) != colour) return;
       const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
-      xw[c] = (L.b[c] - off) * L.inv[c];
+      L.x[c] = (L.b[c] - off) * L.inv[c];
     });
     return;
   }
   const int half = L.NI >> 1;
   const int count = rows * half;
-#pragma unroll 2
-  for (int m = s.tid; m < count; m += s.T) {
+  auto cellOf = [&](int m, int& c, int& i, int& j) {
     const int jj = m / half;
-    const int j = s.j0 + jj;
-    const int i = 2 * (m - jj * half) + ((colour + j) & 1);
-    const int c = j * L.NI + i;
+    j = s.j0 + jj;
+    i = 2 * (m - jj * half) + ((colour + j) & 1);
+    c = j * L.NI + i;
+  };
+  auto value = [&](int c, int i, int j) {
     const float off = kProlonged ? offSumProlonged(L, ec, NIc, c, i, j) : offSum(L, L.x, c, i, j);
-    xw[c] = (L.b[c] - off) * L.inv[c];
+    return (L.b[c] - off) * L.inv[c];
+  };
+  // two cells per step, both computed before either is stored, so their
+  // loads overlap (a store to x could alias the other cell's loads)
+  for (int m = s.tid; m < count; m += 2 * s.T) {
+    int cA, iA, jA;
+    cellOf(m, cA, iA, jA);
+    const float vA = value(cA, iA, jA);
+    const int mB = m + s.T;
+    if (mB < count) {
+      int cB, iB, jB;
+      cellOf(mB, cB, iB, jB);
+      const float vB = value(cB, iB, jB);
+      L.x[cA] = vA;
+      L.x[cB] = vB;
+    } else {
+      L.x[cA] = vA;
+    }
   }
 }
 
@@ -486,29 +503,38 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
       double dq[1] = {0.0};
       const float fb = static_cast<float>(beta);
       {
-      const float* __restrict__ zR = zc;
-      const float* __restrict__ dR = dc;
-      float* __restrict__ dW = dn;
-      float* __restrict__ qW = q;
-#pragma unroll 2
-      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        const int j = c / NI, i = c - j * NI;
-        auto dir = [&](int n) { return (it == 0) ? zR[n] : zR[n] + fb * dR[n]; };
-        const float dv = dir(c);
-        dW[c] = dv;
-        float y = F0.D[c] * dv;
-        if (j > 0) {
-          y += F0.S[c] * dir(c - NI);
-        } else {
-          const int a = I.acrossJ0[i];
-          if (a >= 0) y += F0.S[c] * dir(a);
+        auto dir = [&](int n) { return (it == 0) ? zc[n] : zc[n] + fb * dc[n]; };
+        auto row = [&](int c, float& dv) {
+          const int j = c / NI, i = c - j * NI;
+          dv = dir(c);
+          float y = F0.D[c] * dv;
+          if (j > 0) {
+            y += F0.S[c] * dir(c - NI);
+          } else {
+            const int a = I.acrossJ0[i];
+            if (a >= 0) y += F0.S[c] * dir(a);
+          }
+          if (j < NJ - 1) y += F0.N[c] * dir(c + NI);
+          if (i > 0) y += F0.W[c] * dir(c - 1);
+          if (i < NI - 1) y += F0.E[c] * dir(c + 1);
+          return y;
+        };
+        // two cells per step, loads before stores
+        for (int c = t.c0 + t.tid; c < t.c1; c += 2 * t.T) {
+          float dvA, dvB = 0.0f;
+          const float yA = row(c, dvA);
+          const int cB = c + t.T;
+          const bool hasB = cB < t.c1;
+          const float yB = hasB ? row(cB, dvB) : 0.0f;
+          dn[c] = dvA;
+          q[c] = yA;
+          dq[0] += static_cast<double>(dvA) * static_cast<double>(yA);
+          if (hasB) {
+            dn[cB] = dvB;
+            q[cB] = yB;
+            dq[0] += static_cast<double>(dvB) * static_cast<double>(yB);
+          }
         }
-        if (j < NJ - 1) y += F0.N[c] * dir(c + NI);
-        if (i > 0) y += F0.W[c] * dir(c - 1);
-        if (i < NI - 1) y += F0.E[c] * dir(c + 1);
-        qW[c] = y;
-        dq[0] += static_cast<double>(dv) * static_cast<double>(y);
-      }
       }
       {
         float* tmp = dc;
@@ -520,20 +546,27 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
       const float alpha = static_cast<float>(rz / dq[0]);
       double v3[3] = {0.0, 0.0, 0.0};
       {
-      float* __restrict__ eW = e;
-      float* __restrict__ rW = r;
-      float* __restrict__ zW = zp;
-      const float* __restrict__ dR = dc;
-      const float* __restrict__ qR = q;
-#pragma unroll 2
-      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        const int j = c / NI, i = c - j * NI;
-        eW[c] += alpha * dR[c];
-        const float rc = rW[c] - alpha * qR[c];
-        rW[c] = rc;
-        v3[2] += fabs(static_cast<double>(rc));
-        zW[c] = (((i + j) & 1) == 0) ? rc * F0.inv[c] : 0.0f;
-      }
+        // e += alpha d, r -= alpha q, and the next V-cycle's red start
+        // z = r / D; two cells per step, loads before stores
+        auto upd = [&](int c, float& ev, float& rv, float& zv) {
+          const int j = c / NI, i = c - j * NI;
+          ev = e[c] + alpha * dc[c];
+          rv = r[c] - alpha * q[c];
+          zv = (((i + j) & 1) == 0) ? rv * F0.inv[c] : 0.0f;
+        };
+        for (int c = t.c0 + t.tid; c < t.c1; c += 2 * t.T) {
+          float eA, rA, zA, eB = 0.0f, rB = 0.0f, zB = 0.0f;
+          upd(c, eA, rA, zA);
+          const int cB = c + t.T;
+          const bool hasB = cB < t.c1;
+          if (hasB) upd(cB, eB, rB, zB);
+          e[c] = eA; r[c] = rA; zp[c] = zA;
+          v3[2] += fabs(static_cast<double>(rA));
+          if (hasB) {
+            e[cB] = eB; r[cB] = rB; zp[cB] = zB;
+            v3[2] += fabs(static_cast<double>(rB));
+          }
+        }
       }
       ++total;
       vcycle(G, t, smem, zp);
@@ -541,20 +574,30 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
         Lv Z = F0;
         Z.x = zp;
         Z.b = r;
-        float* __restrict__ zW = zp;
-#pragma unroll 2
-        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        // the last red half sweep of the V-cycle, fused with r.z_new and
+        // r.z_old; two cells per step, loads before stores
+        auto fin = [&](int c, float& zv, bool& red) {
           const int j = c / NI, i = c - j * NI;
-          float zv;
-          if (((i + j) & 1) == 0) {
-            zv = (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c];
-            zW[c] = zv;
-          } else {
-            zv = zp[c];
+          red = ((i + j) & 1) == 0;
+          zv = red ? (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c] : zp[c];
+        };
+        for (int c = t.c0 + t.tid; c < t.c1; c += 2 * t.T) {
+          float zA, zB = 0.0f;
+          bool redA, redB = false;
+          fin(c, zA, redA);
+          const int cB = c + t.T;
+          const bool hasB = cB < t.c1;
+          if (hasB) fin(cB, zB, redB);
+          const double rA = static_cast<double>(r[c]);
+          v3[0] += rA * static_cast<double>(zA);
+          v3[1] += rA * static_cast<double>(zc[c]);
+          if (hasB) {
+            const double rB = static_cast<double>(r[cB]);
+            v3[0] += rB * static_cast<double>(zB);
+            v3[1] += rB * static_cast<double>(zc[cB]);
           }
-          const double rc = static_cast<double>(r[c]);
-          v3[0] += rc * static_cast<double>(zv);
-          v3[1] += rc * static_cast<double>(zc[c]);
+          if (redA) zp[c] = zA;
+          if (hasB && redB) zp[cB] = zB;
         }
       }
       teamReduce(t, sh, v3, op3);
