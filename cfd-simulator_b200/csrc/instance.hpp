@@ -78,6 +78,7 @@ struct MgLevel {
   float *x, *b;              // iterate and right-hand side (global memory)
   const int* wake;           // partner column across j = 0, or -1
   int smem;                  // byte offset of the level in shared memory when rank 0 runs it alone
+  int smemWake;              // byte offset of its wake map there
 };
 
 struct Multigrid {

@@ -50,11 +50,12 @@ DEV Lv globalLevel(const MgLevel& M) {
 }
 
 /// Eight arrays of the level in shared memory from byte offset M.smem, each
-/// rounded up to 4 floats.
+/// rounded up to 4 floats, and its wake map from M.smemWake.
 DEV Lv sharedLevel(const MgLevel& M, char* smem) {
   float* p = reinterpret_cast<float*>(smem + M.smem);
   const int n = (M.NI * M.NJ + 3) & ~3;
-  return Lv{M.NI, M.NJ, p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, p + 6 * n, p + 7 * n, M.wake};
+  return Lv{M.NI, M.NJ, p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, p + 6 * n, p + 7 * n,
+            reinterpret_cast<const int*>(smem + M.smemWake)};
 }
 
 DEV Lv levelView(const Multigrid& G, int l, char* smem) {
@@ -100,36 +101,44 @@ DEV void forColour(const Lv& L, const Span& s, int colour, F&& f) {
   }
 }
 
+/// Neighbour indices of cell (i, j) for branch-free row products: a missing
+/// neighbour is replaced by the cell itself, whose coefficient on that side
+/// is zero on every level (the fine rows are built that way and the Galerkin
+/// sums only ever add existing couplings), so every load can be issued
+/// unconditionally and together.
+struct Nbrs {
+  int s, n, w, e;
+};
+DEV Nbrs neighbours(const int* wake, int NI, int NJ, int c, int i, int j) {
+  const int a = wake[i];
+  Nbrs q;
+  q.s = (j > 0) ? c - NI : ((a >= 0) ? a : c);
+  q.n = (j < NJ - 1) ? c + NI : c;
+  q.w = (i > 0) ? c - 1 : c;
+  q.e = (i < NI - 1) ? c + 1 : c;
+  return q;
+}
+
 /// Off-diagonal part of row c applied to x (S, N, W, E).
 DEV float offSum(const Lv& L, const float* x, int c, int i, int j) {
-  float s = 0.0f;
-  if (j > 0) {
-    s += L.S[c] * x[c - L.NI];
-  } else {
-    const int a = L.wake[i];
-    if (a >= 0) s += L.S[c] * x[a];
-  }
-  if (j < L.NJ - 1) s += L.N[c] * x[c + L.NI];
-  if (i > 0) s += L.W[c] * x[c - 1];
-  if (i < L.NI - 1) s += L.E[c] * x[c + 1];
-  return s;
+  const Nbrs q = neighbours(L.wake, L.NI, L.NJ, c, i, j);
+  return L.S[c] * x[q.s] + L.N[c] * x[q.n] + L.W[c] * x[q.w] + L.E[c] * x[q.e];
 }
 
 /// The same with every neighbour's value corrected by its aggregate's value
-/// on the next coarser level (piecewise-constant prolongation).
+/// on the next coarser level (piecewise-constant prolongation). The
+/// aggregates follow from (i, j) directly; a missing neighbour (the cell
+/// itself, zero coefficient) uses the cell's own aggregate.
 DEV float offSumProlonged(const Lv& L, const float* ec, int NIc, int c, int i, int j) {
-  auto val = [&](int n, int ni, int nj) { return L.x[n] + ec[(nj >> 1) * NIc + (ni >> 1)]; };
-  float s = 0.0f;
-  if (j > 0) {
-    s += L.S[c] * val(c - L.NI, i, j - 1);
-  } else {
-    const int a = L.wake[i];
-    if (a >= 0) s += L.S[c] * val(a, a, 0);
-  }
-  if (j < L.NJ - 1) s += L.N[c] * val(c + L.NI, i, j + 1);
-  if (i > 0) s += L.W[c] * val(c - 1, i - 1, j);
-  if (i < L.NI - 1) s += L.E[c] * val(c + 1, i + 1, j);
-  return s;
+  const Nbrs q = neighbours(L.wake, L.NI, L.NJ, c, i, j);
+  const int own = (j >> 1) * NIc + (i >> 1);
+  const int a = L.wake[i];
+  const int gS = (j > 0) ? ((j - 1) >> 1) * NIc + (i >> 1) : ((a >= 0) ? (a >> 1) : own);
+  const int gN = (j < L.NJ - 1) ? ((j + 1) >> 1) * NIc + (i >> 1) : own;
+  const int gW = (i > 0) ? (j >> 1) * NIc + ((i - 1) >> 1) : own;
+  const int gE = (i < L.NI - 1) ? (j >> 1) * NIc + ((i + 1) >> 1) : own;
+  return L.S[c] * (L.x[q.s] + ec[gS]) + L.N[c] * (L.x[q.n] + ec[gN]) +
+         L.W[c] * (L.x[q.w] + ec[gW]) + L.E[c] * (L.x[q.e] + ec[gE]);
 }
 
 /// Gauss-Seidel half sweep over the cells of one colour. The new values are
@@ -457,6 +466,11 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
   t.cl.sync();
   if (G.distributed < G.levels && t.rank == 0) {
     for (int l = G.distributed; l < G.levels; ++l) {
+      int* w = reinterpret_cast<int*>(smem + G.lv[l].smemWake);
+      for (int i = t.tid; i < G.lv[l].NI; i += t.T) w[i] = G.lv[l].wake[i];
+    }
+    __syncthreads();
+    for (int l = G.distributed; l < G.levels; ++l) {
       if (l > G.distributed) __syncthreads();
       const Lv C = sharedLevel(G.lv[l], smem);
       galerkin(levelView(G, l - 1, smem), C, wholeOf(C));
@@ -506,18 +520,10 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
         auto dir = [&](int n) { return (it == 0) ? zc[n] : zc[n] + fb * dc[n]; };
         auto row = [&](int c, float& dv) {
           const int j = c / NI, i = c - j * NI;
+          const Nbrs nb = neighbours(F0.wake, NI, NJ, c, i, j);
           dv = dir(c);
-          float y = F0.D[c] * dv;
-          if (j > 0) {
-            y += F0.S[c] * dir(c - NI);
-          } else {
-            const int a = I.acrossJ0[i];
-            if (a >= 0) y += F0.S[c] * dir(a);
-          }
-          if (j < NJ - 1) y += F0.N[c] * dir(c + NI);
-          if (i > 0) y += F0.W[c] * dir(c - 1);
-          if (i < NI - 1) y += F0.E[c] * dir(c + 1);
-          return y;
+          return F0.D[c] * dv + F0.S[c] * dir(nb.s) + F0.N[c] * dir(nb.n) + F0.W[c] * dir(nb.w) +
+                 F0.E[c] * dir(nb.e);
         };
         // two cells per step, loads before stores
         for (int c = t.c0 + t.tid; c < t.c1; c += 2 * t.T) {
@@ -575,29 +581,15 @@ __device__ __noinline__ int pressureMixed(const Instance& I, Team& t, Shared& sh
         Z.x = zp;
         Z.b = r;
         // the last red half sweep of the V-cycle, fused with r.z_new and
-        // r.z_old; two cells per step, loads before stores
-        auto fin = [&](int c, float& zv, bool& red) {
-          const int j = c / NI, i = c - j * NI;
-          red = ((i + j) & 1) == 0;
-          zv = red ? (r[c] - offSum(Z, zp, c, i, j)) * Z.inv[c] : zp[c];
-        };
-        for (int c = t.c0 + t.tid; c < t.c1; c += 2 * t.T) {
-          float zA, zB = 0.0f;
-          bool redA, redB = false;
-          fin(c, zA, redA);
-          const int cB = c + t.T;
-          const bool hasB = cB < t.c1;
-          if (hasB) fin(cB, zB, redB);
-          const double rA = static_cast<double>(r[c]);
-          v3[0] += rA * static_cast<double>(zA);
-          v3[1] += rA * static_cast<double>(zc[c]);
-          if (hasB) {
-            const double rB = static_cast<double>(r[cB]);
-            v3[0] += rB * static_cast<double>(zB);
-            v3[1] += rB * static_cast<double>(zc[cB]);
-          }
-          if (redA) zp[c] = zA;
-          if (hasB && redB) zp[cB] = zB;
+        // r.z_old: red cells first (with their update), then black ones, so
+        // no warp diverges on the colour
+        const Span band = bandOf(Z, t);
+        sweepCells<false>(Z, band, 0, nullptr, 0);
+        __syncthreads();  // the dot products read every red cell of the band
+        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+          const double rc = static_cast<double>(r[c]);
+          v3[0] += rc * static_cast<double>(zp[c]);
+          v3[1] += rc * static_cast<double>(zc[c]);
         }
       }
       teamReduce(t, sh, v3, op3);

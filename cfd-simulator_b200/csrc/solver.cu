@@ -367,6 +367,7 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
         L.NI = sh.NI;
         L.NJ = sh.NJ;
         L.smem = sh.smem;
+        L.smemWake = sh.smemWake;
         L.D = a.take<float>(n); L.S = a.take<float>(n); L.N = a.take<float>(n);
         L.W = a.take<float>(n); L.E = a.take<float>(n); L.inv = a.take<float>(n);
         L.x = a.take<float>(n); L.b = a.take<float>(n);
@@ -489,13 +490,13 @@ std::size_t Solver::estimateBytes(int NI, int NJ) {
 
 void Solver::planMultigrid(const std::vector<int>& wake0) {
   mgShape_.clear();
-  mgShape_.push_back(MgShape{NI_, NJ_, -1, wake0});
+  mgShape_.push_back(MgShape{NI_, NJ_, -1, -1, wake0});
   // Halve both directions while the columns pair up and the wake map stays
   // a map between aggregates (partner aggregates of the two cells agree).
   while (static_cast<int>(mgShape_.size()) < kMaxMgLevels) {
     const MgShape f = mgShape_.back();
     if (f.NI % 2 != 0 || f.NJ < 2 || f.NI * f.NJ <= 16) break;
-    MgShape c{f.NI / 2, (f.NJ + 1) / 2, -1, std::vector<int>(f.NI / 2, -1)};
+    MgShape c{f.NI / 2, (f.NJ + 1) / 2, -1, -1, std::vector<int>(f.NI / 2, -1)};
     bool ok = true;
     for (int I = 0; I < c.NI; ++I) {
       const int a = f.wake[2 * I], b = f.wake[2 * I + 1];
@@ -519,6 +520,8 @@ void Solver::planMultigrid(const std::vector<int>& wake0) {
   for (int l = mgDistributed_; l < levels; ++l) {
     mgShape_[l].smem = bytes;
     bytes += 8 * ((mgShape_[l].NI * mgShape_[l].NJ + 3) & ~3) * static_cast<int>(sizeof(float));
+    mgShape_[l].smemWake = bytes;
+    bytes += ((mgShape_[l].NI + 3) & ~3) * static_cast<int>(sizeof(int));
   }
   mgSmemBytes_ = bytes;
 }

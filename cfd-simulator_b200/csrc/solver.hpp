@@ -161,7 +161,7 @@ class Solver {
   int threads_{512};
 
   struct MgShape {
-    int NI, NJ, smem;
+    int NI, NJ, smem, smemWake;
     std::vector<int> wake;
   };
   std::vector<MgShape> mgShape_;
