@@ -193,6 +193,7 @@ _sig("cfd_engine_submit", C.c_int, _P, _P, _P)
 _sig("cfd_engine_step", C.c_int, _P, _P, _P)
 _sig("cfd_engine_results", C.c_int, _P, _P, C.c_int, _P)
 _sig("cfd_engine_surface", C.c_int, _P, C.c_int, _P, C.c_int, _P)
+_sig("cfd_engine_set_shape_policy", C.c_int, _P, C.c_int)
 _sig("cfd_engine_clock", C.c_double, _P)
 _sig("cfd_engine_destroy", C.c_int, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
@@ -578,9 +579,11 @@ def request(designation: str, alpha_deg: float, reynolds: float, model: int = MO
 class Engine:
     """Continuous batching of many solves (cfd_engine_*)."""
 
-    def __init__(self, memory_budget_bytes: int = 0, chunk: int = 32):
+    def __init__(self, memory_budget_bytes: int = 0, chunk: int = 32, tuned: bool = False):
         self._h = C.c_void_p()
         _check(_lib.cfd_engine_create(memory_budget_bytes, chunk, C.byref(self._h)))
+        if tuned:
+            _check(_lib.cfd_engine_set_shape_policy(self._h, 1))
 
     def close(self) -> None:
         if self._h:

@@ -80,6 +80,7 @@ std::mutex g_shapesMutex;
 struct Engine {
   std::size_t budget{0};
   std::size_t used{0};
+  bool tuned{false};  // launch shapes: by grid size (false) or the occupancy tuner (true)
   int chunk{32};
   int nextId{0};
   std::deque<Pending> queue;
@@ -171,6 +172,10 @@ struct Engine {
   /// the same bits, whatever else is in the engine. CFD_ENGINE_TUNE=0 keeps the solver's
   /// default shape.
   Status tunedShape(const Pending& q, const Solver& s, std::pair<int, int>* out) {
+    if (!tuned) {
+      *out = {s.clusterSize(), s.threads()};
+      return ok();
+    }
     const auto key = std::make_tuple(s.cellsI(), s.cellsJ(), q.request.model, s.precision());
     std::lock_guard<std::mutex> lock(g_shapesMutex);
     if (auto it = g_shapes.find(key); it != g_shapes.end()) {
@@ -515,6 +520,13 @@ cfd_status cfd_engine_surface(cfd_engine e, int id, double* cp, int capacity, in
   if (capacity < n) return cfdb::fail(CFD_INVALID_ARGUMENT, "cp buffer too small");
   std::copy(it->second.begin(), it->second.end(), cp);
   g.surfaces.erase(it);
+  return CFD_OK;
+}
+
+cfd_status cfd_engine_set_shape_policy(cfd_engine e, int policy) {
+  if (e == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null engine");
+  if (policy != 0 && policy != 1) return cfdb::fail(CFD_INVALID_ARGUMENT, "policy must be 0 or 1");
+  e->engine.tuned = (policy == 1);
   return CFD_OK;
 }
 

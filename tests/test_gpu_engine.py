@@ -109,6 +109,19 @@ def test_iteration_limit_is_reported():
 
 def test_tuned_shape_is_fixed_per_grid_and_reported():
     reqs = [_req(alpha=a, tol=1e-5, cap=200) for a in (0.0, 2.0)]
-    res = cb.Engine(chunk=32).run(reqs)
+    res = cb.Engine(chunk=32, tuned=True).run(reqs)
     shapes = {r.cluster_size for r in res}
-    assert len(shapes) == 1 and shapes.pop() in (4, 6, 8, 16)
+    assert len(shapes) == 1 and shapes.pop() in (4, 8, 16)
+    # the same grid in another tuned engine of the process: the same shape
+    again = cb.Engine(chunk=32, tuned=True).run(reqs[:1])[0]
+    assert again.cluster_size == res[0].cluster_size
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix_when_tuned():
+    mix = [_req(alpha=4.0, tol=1e-6), _req("0015", alpha=-3.0, re=2e5, tol=1e-6,
+                                            grid=dict(surface_points=20, wake_points=8, normal_points=9))]
+    together = cb.Engine(chunk=16, tuned=True).run(mix)
+    for k, req in enumerate(mix):
+        a, b = cb.Engine(chunk=16, tuned=True).run([req])[0], together[k]
+        assert (a.status, a.iterations, a.cluster_size) == (b.status, b.iterations, b.cluster_size)
+        assert a.lift_coefficient == pytest.approx(b.lift_coefficient, rel=1e-12, abs=1e-15)
