@@ -177,10 +177,10 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def committed_traffic() -> float | None:
+def committed_traffic(name: str = "simple_kernel_c2_sst_fp64.md") -> float | None:
     """DRAM bytes per launch of simpleKernel on this workload, from the
     committed ncu summary (its `traffic_bytes_per_launch:` line)."""
-    path = os.path.join(ROOT, "profiles", "simple_kernel_c2_sst_fp64.md")
+    path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
             for line in f:
@@ -287,7 +287,8 @@ def run_ours(args) -> None:
 
     import cfd_b200 as cb
     cb.set_device(torch.cuda.current_device())
-    mesh, solvers = build_solvers(cb)
+    mixed = args.form == "mixed"
+    mesh, solvers = build_solvers(cb, 1 if mixed else 0)
     batch = cb.Batch(solvers)
     cells = mesh.cells * len(solvers)
     # A stream of our own: events, the L2 flush and the solver launches all go
@@ -371,10 +372,13 @@ def run_ours(args) -> None:
     if rank == 0:
         import bytes_model
         peak, peak_kind = measured_peak()
-        per_launch_bytes = bytes_model.bytes_per_cell_iteration(True, mean_cg) * cells
+        if mixed:
+            per_launch_bytes = bytes_model.bytes_per_cell_iteration_mixed(True, mean_cg) * cells
+        else:
+            per_launch_bytes = bytes_model.bytes_per_cell_iteration(True, mean_cg) * cells
         mean_launch_s = float(np.mean(step_ms)) / 1e3
         achieved = per_launch_bytes / mean_launch_s / 1e9
-        traffic = committed_traffic()
+        traffic = committed_traffic("simple_kernel_c2_sst_mixed.md" if mixed else "simple_kernel_c2_sst_fp64.md")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                     "traffic": traffic,
@@ -383,8 +387,14 @@ def run_ours(args) -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config({"cluster_shape": list(batch.shape())}),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64" if mixed else "f64",
+            "data": "synthetic",
+            "config": config({"cluster_shape": list(batch.shape())} if not mixed else
+                             {"cluster_shape": list(batch.shape()),
+                              "workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 "
+                                          "and 4 deg, mixed FP32/FP64 form, batched in one launch",
+                              "precision": "mixed: FP64 assembly/state, FP32 sweeps and multigrid CG"}),
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -628,6 +638,8 @@ def main() -> None:
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
+                    help="c2: the form the benchmark line times (plain FP64 by default)")
     ap.add_argument("--precision", choices=("plain", "mixed", "both"), default="both",
                     help="polar: which form(s) to run; serve: plain unless 'mixed'")
     args = ap.parse_args()

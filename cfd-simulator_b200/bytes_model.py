@@ -29,3 +29,25 @@ CG_ACCESSES = 12
 def bytes_per_cell_iteration(sst: bool, mean_cg_iterations: float, width: int = 8) -> float:
     a_outer = A_OUTER_SST if sst else A_OUTER_LAMINAR
     return float(width) * (a_outer + CG_ACCESSES * mean_cg_iterations)
+
+
+# The mixed FP32/FP64 form: the outer stages as above (assembly and state in
+# FP64, 8 B), plus per inner (multigrid-CG) iteration, in FP32 (4 B):
+#   flexible CG 20 accesses per cell: A d' (z and d, five coefficients,
+#   write d and q: 9), the update (e, d, r, q, 1/D; write e, r, z: 8), the
+#   dot products (r, z, z_old: 3);
+#   one V-cycle 40 per fine cell: on the fine level a black half sweep
+#   before (5.5: six row values and four neighbours per black cell, write),
+#   the residual restriction (11.5), the black half sweep after with the
+#   coarse correction (7.5) and the last red one (5.5), 30 together, and a
+#   third of that again for all coarser levels;
+# and per outer iteration 12 FP64 accesses for the refinement (x += e;
+# r = b - A x) and 9 for the FP32 copy of the pressure-correction rows.
+MG_CG_ACCESSES = 20
+MG_VCYCLE_ACCESSES = 40
+MG_OUTER_FP64 = 12 + 9
+
+
+def bytes_per_cell_iteration_mixed(sst: bool, mean_inner_iterations: float) -> float:
+    a_outer = A_OUTER_SST if sst else A_OUTER_LAMINAR
+    return 8.0 * (a_outer + MG_OUTER_FP64) + 4.0 * (MG_CG_ACCESSES + MG_VCYCLE_ACCESSES) * mean_inner_iterations
