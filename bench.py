@@ -300,9 +300,10 @@ def run_ours(args) -> None:
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     # warm-up (untimed), also moves the flow off its uniform start
+    launch = batch.graph_launch if args.graph else batch.launch
     for _ in range(args.warmup):
         flush.zero_()
-        batch.launch(1, handle)
+        launch(1, handle)
     torch.cuda.synchronize()
 
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -314,7 +315,7 @@ def run_ours(args) -> None:
         for k in range(args.steps):
             flush.zero_()
             starts[k].record(stream)
-            batch.launch(1, handle)
+            launch(1, handle)
             ends[k].record(stream)
         torch.cuda.synchronize()
     if dist is not None:
@@ -390,7 +391,8 @@ def run_ours(args) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64" if mixed else "f64",
             "data": "synthetic",
-            "config": config({"cluster_shape": list(batch.shape())} if not mixed else
+            "config": config({"cluster_shape": list(batch.shape()), "launch": "cuda graph" if args.graph else "direct"}
+                             if not mixed else
                              {"cluster_shape": list(batch.shape()),
                               "workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 "
                                           "and 4 deg, mixed FP32/FP64 form, batched in one launch",
@@ -638,6 +640,8 @@ def main() -> None:
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--graph", action="store_true",
+                    help="c2: replay each step's launch from a CUDA graph")
     ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
                     help="c2: the form the benchmark line times (plain FP64 by default)")
     ap.add_argument("--precision", choices=("plain", "mixed", "both"), default="both",

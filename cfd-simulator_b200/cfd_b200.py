@@ -199,6 +199,7 @@ _sig("cfd_engine_destroy", C.c_int, _P)
 _sig("cfd_batch_create", C.c_int, _P, C.c_int, _P)
 _sig("cfd_batch_iterate", C.c_int, _P, C.c_int, C.c_double, _P, _P)
 _sig("cfd_batch_launch", C.c_int, _P, C.c_int, _P)
+_sig("cfd_batch_graph_launch", C.c_int, _P, C.c_int, _P)
 _sig("cfd_batch_monitors", C.c_int, _P, _P, _P)
 _sig("cfd_batch_shape", C.c_int, _P, _P, _P)
 _sig("cfd_batch_destroy", C.c_int, _P)
@@ -517,6 +518,10 @@ class Batch:
     def launch(self, n: int, stream: int | None = None) -> None:
         """Enqueue n iterations on a CUDA stream (an int handle) without waiting."""
         _check(_lib.cfd_batch_launch(self._h, n, None if stream is None else C.c_void_p(stream)))
+
+    def graph_launch(self, n: int, stream: int | None = None) -> None:
+        """The same, replayed from a CUDA graph captured on first use."""
+        _check(_lib.cfd_batch_graph_launch(self._h, n, None if stream is None else C.c_void_p(stream)))
 
     def monitors(self):
         count = len(self.solvers)

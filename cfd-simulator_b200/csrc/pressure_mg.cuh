@@ -321,7 +321,6 @@ DEV void sharedCycle(const Multigrid& G, char* smem) {
       C.x[c] = (((i + j) & 1) == 0) ? b * C.inv[c] : 0.0f;
     });
   }
-  auto block = [] { __syncthreads(); };
   auto warp = [] { __syncwarp(); };
   if (w == m) {
     // every shared level is small: warp 0 runs them all
@@ -363,7 +362,6 @@ DEV void sharedCycle(const Multigrid& G, char* smem) {
       }
     }
   }
-  (void)block;
   __syncthreads();
   const Lv A = sharedLevel(G.lv[m], smem);
   float* out = G.lv[m].x;

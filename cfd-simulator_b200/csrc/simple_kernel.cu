@@ -1538,6 +1538,8 @@ Status configureSimpleKernel() {
 
 }  // namespace
 
+Status prepareSimpleKernel() { return configureSimpleKernel(); }
+
 int maxActiveClusters(int clusterSize, int threads, int smemBytes) {
   if (configureSimpleKernel() != CFD_OK) return 0;
   cudaLaunchConfig_t config = {};

@@ -1175,6 +1175,8 @@ struct cfd_batch_t {
   int threads{512};
   int smemBytes{0};
   int lastIterations{0};
+  cudaGraphExec_t graph{nullptr};  // the n-iteration launch, captured once
+  int graphIterations{0};
 };
 
 namespace {
@@ -1231,6 +1233,44 @@ cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream) {
   b->lastIterations = n;
   return cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize, b->threads, n,
                             cfdb::kStageEnd, -1.0, s, b->smemBytes);
+}
+
+cfd_status cfd_batch_graph_launch(cfd_batch b, int n, void* stream) {
+  if (b == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null batch");
+  if (n < 1 || n > 256) return cfdb::fail(CFD_OUT_OF_RANGE, "a batch launch runs 1 to 256 iterations");
+  for (cfd_handle h : b->handles) {
+    if (!h->solver->initialised()) return cfdb::fail(CFD_INVALID_ARGUMENT, "a solver in the batch is not initialised");
+  }
+  if (b->graph == nullptr || b->graphIterations != n) {
+    if (b->graph != nullptr) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    if (cfd_status st = cfdb::prepareSimpleKernel(); st != CFD_OK) return st;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    const cfd_status launched = cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize,
+                                                   b->threads, n, cfdb::kStageEnd, -1.0, b->stream, b->smemBytes);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(b->stream, &g);
+    if (launched != CFD_OK) {
+      if (g != nullptr) cudaGraphDestroy(g);
+      return launched;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->graph, g, 0);
+    if (g != nullptr) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->graph = nullptr;
+      return cfdb::fail(CFD_INITIALIZATION_FAILURE, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    b->graphIterations = n;
+  }
+  cudaStream_t s = (stream != nullptr) ? static_cast<cudaStream_t>(stream) : b->stream;
+  b->lastIterations = n;
+  const cudaError_t e = cudaGraphLaunch(b->graph, s);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  return CFD_OK;
 }
 
 cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last) {
@@ -1294,6 +1334,7 @@ cfd_status cfd_batch_shape(cfd_batch b, int* clusterSize, int* threads) {
 cfd_status cfd_batch_destroy(cfd_batch b) {
   if (b == nullptr) return CFD_OK;
   cudaStreamSynchronize(b->stream);
+  if (b->graph != nullptr) cudaGraphExecDestroy(b->graph);
   cudaFree(b->dTable);
   cudaStreamDestroy(b->stream);
   delete b;

@@ -190,6 +190,10 @@ constexpr int kMaxCgSharedBytes = 210 * 1024;
 /// Cluster size used for a solve of `cells` cells (power of two, 1..16).
 int chooseClusterSize(int cells);
 
+/// Set the kernel's launch attributes (once per process); must run before a
+/// launch is captured into a CUDA graph.
+Status prepareSimpleKernel();
+
 /// Clusters of this shape the GPU holds at once (cudaOccupancyMaxActiveClusters).
 int maxActiveClusters(int clusterSize, int threads, int smemBytes);
 

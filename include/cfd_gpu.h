@@ -344,6 +344,11 @@ cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_mon
  * own stream, not the legacy default stream) and return without waiting;
  * for callers that time with events on their own stream. */
 cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream);
+/* The same launch replayed from a CUDA graph: the n-iteration launch is
+ * captured on the batch's stream the first time (and again when n changes)
+ * and then launched as a graph on `stream` (NULL: the batch's stream). The
+ * results are those of cfd_batch_launch. */
+cfd_status cfd_batch_graph_launch(cfd_batch b, int n, void* stream);
 /* Monitors of the last launch (count entries); synchronises first. */
 cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last);
 /* Cluster size (CTAs per solve) and threads per CTA used by launches. */

@@ -67,3 +67,18 @@ def test_wide_cluster_tracks_the_oracle(name, ctas):
     assert np.max(np.abs(hist[:, 5] - mo[:, 5])) <= 1
     for field, fid in (("U", 0), ("V", 1), ("P", 2), ("K", 22), ("OMEGA", 23), ("MUT", 24)):
         assert rel_err(d.read(field), o.read(fid)) < 1e-7, field
+
+
+def test_graph_replayed_launches_equal_direct_launches():
+    c = Case("sst_cgrid")
+    a, b = c.device(), c.device()
+    ba, bb = cb.Batch([a]), cb.Batch([b])
+    for _ in range(12):
+        ba.launch(1)
+        bb.graph_launch(1)
+    ba.monitors()
+    bb.monitors()
+    for f in FIELDS:
+        assert np.array_equal(a.read(f), b.read(f)), f
+    ba.close()
+    bb.close()
