@@ -22,11 +22,10 @@ DEV double sclamp(double v, double lo, double hi) { return (v < lo) ? lo : ((hi 
 
 constexpr int kMaxWarps = 32;
 constexpr int kRedSlots = 8;
-constexpr int kMaxRanks = 16;
 
 struct Shared {
   double warp[kMaxWarps][kRedSlots];
-  double part[2][kMaxRanks][kRedSlots];  // every rank's partials, pushed here by their owners
+  double part[2][kRedSlots];
   double result[kRedSlots];
 };
 
@@ -47,13 +46,11 @@ DEV double identity(int op) { return (op == kMax) ? -INFINITY : 0.0; }
 
 /// Reduce K values over every thread of the cluster. The result is the same
 /// bits in every thread of every CTA: a fixed warp tree, the warp partials
-/// in warp order, then each CTA's partial is pushed into every CTA's shared
-/// memory (one remote store per rank, before the barrier) and, after the
-/// barrier, warp 0 reduces the ranks' partials in rank order with the same
-/// tree from its own shared memory. Contains two __syncthreads and one
-/// cluster barrier. (Having every warp read the ranks' partials instead, to
-/// drop the second __syncthreads, measured 0.65 us slower per reduction at
-/// 16 CTAs; reading them remotely after the barrier, ~0.2 us slower.)
+/// in warp order, then warp 0 reads the ranks' partials in rank order from
+/// distributed shared memory and reduces them with the same tree.
+/// Contains two __syncthreads and one cluster barrier. (Having every warp
+/// read the ranks' partials instead, to drop the second __syncthreads,
+/// measured 0.65 us slower per reduction at 16 CTAs.)
 template <int K>
 DEV void teamReduce(Team& t, Shared& sh, double (&v)[K], const int (&op)[K]) {
   const int lane = threadIdx.x & 31;
@@ -77,8 +74,7 @@ DEV void teamReduce(Team& t, Shared& sh, double (&v)[K], const int (&op)[K]) {
       double a = (lane < nwarps) ? sh.warp[lane][k] : identity(op[k]);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
-      const double mine = __shfl_sync(0xffffffffu, a, 0);
-      if (lane < static_cast<int>(t.R)) *t.cl.map_shared_rank(&sh.part[t.buf][t.rank][k], lane) = mine;
+      if (lane == 0) sh.part[t.buf][k] = a;
     }
   }
   t.cl.sync();
@@ -86,7 +82,7 @@ DEV void teamReduce(Team& t, Shared& sh, double (&v)[K], const int (&op)[K]) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       double a = identity(op[k]);
-      if (lane < static_cast<int>(t.R)) a = sh.part[t.buf][lane][k];
+      if (lane < static_cast<int>(t.R)) a = *t.cl.map_shared_rank(&sh.part[t.buf][k], lane);
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) a = combine(op[k], a, __shfl_down_sync(0xffffffffu, a, off));
       if (lane == 0) sh.result[k] = a;
