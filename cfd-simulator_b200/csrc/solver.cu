@@ -333,6 +333,7 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     dWall_.wallDistance = a.take<double>(S);
     dWall_.outerDistance = a.take<double>(S);
     dStations_ = a.take<double>(S * kStationValues);
+    dFaceStage_ = a.take<double>(static_cast<std::size_t>(F_));
     dForces_ = a.take<double>(16);
     if (!mgShape_.empty()) {
       Multigrid& G = I.mg;
@@ -963,26 +964,52 @@ Status Solver::forces(double speed, double alphaDeg, double density, double refe
   return CFD_OK;
 }
 
+namespace {
+
+/// Reference face order -> the two device families: j-faces keep their
+/// index, i-face offset + i*NJ + j goes to j*(NI+1) + i.
+__global__ void scatterFacesKernel(const double* __restrict__ src, double* __restrict__ n,
+                                   double* __restrict__ e, int NI, int NJ) {
+  const int jFaces = NI * (NJ + 1);
+  const int F = jFaces + (NI + 1) * NJ;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < F; f += gridDim.x * blockDim.x) {
+    if (f < jFaces) {
+      n[f] = src[f];
+    } else {
+      const int g = f - jFaces, i = g / NJ, j = g - i * NJ;
+      e[j * (NI + 1) + i] = src[f];
+    }
+  }
+}
+
+}  // namespace
+
 Status Solver::loadState(const double* u, const double* v, const double* p, const double* massFlux,
                          const double* k, const double* omega, const double* mut, const double* muEff) {
   if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
   const Instance& I = view_;
-  const std::size_t N = N_;
-  Status st = CFD_OK;
-  if (u != nullptr && (st = upload(I.u, u, N))) return st;
-  if (v != nullptr && (st = upload(I.v, v, N))) return st;
-  if (p != nullptr && (st = upload(I.p, p, N))) return st;
+  const std::size_t bytes = static_cast<std::size_t>(N_) * sizeof(double);
+  // One wait for the solver's own work, then every copy queued on its
+  // stream (the face permutation runs on the device), then one wait so the
+  // caller may reuse its buffers on return.
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
+  auto put = [&](double* dev, const double* host) -> cudaError_t {
+    return (host == nullptr) ? cudaSuccess : cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, stream_);
+  };
+  CUDA_OR_FAIL(put(I.u, u));
+  CUDA_OR_FAIL(put(I.v, v));
+  CUDA_OR_FAIL(put(I.p, p));
+  CUDA_OR_FAIL(put(I.k, k));
+  CUDA_OR_FAIL(put(I.om, omega));
+  CUDA_OR_FAIL(put(I.mut, mut));
+  CUDA_OR_FAIL(put(I.mu, muEff));
   if (massFlux != nullptr) {
-    const std::size_t FN = static_cast<std::size_t>(NI_) * (NJ_ + 1);
-    const std::size_t FE = static_cast<std::size_t>(NI_ + 1) * NJ_;
-    std::vector<double> hN(FN, 0.0), hE(FE, 0.0);
-    for (int f = 0; f < F_; ++f) (famOf(f) ? hE : hN)[idxOf(f)] = massFlux[f];
-    if ((st = upload(I.mfN, hN.data(), FN)) || (st = upload(I.mfE, hE.data(), FE))) return st;
+    CUDA_OR_FAIL(cudaMemcpyAsync(dFaceStage_, massFlux, static_cast<std::size_t>(F_) * sizeof(double),
+                                 cudaMemcpyHostToDevice, stream_));
+    scatterFacesKernel<<<std::min((F_ + 255) / 256, 1024), 256, 0, stream_>>>(dFaceStage_, I.mfN, I.mfE, NI_, NJ_);
+    CUDA_OR_FAIL(cudaGetLastError());
   }
-  if (k != nullptr && (st = upload(I.k, k, N))) return st;
-  if (omega != nullptr && (st = upload(I.om, omega, N))) return st;
-  if (mut != nullptr && (st = upload(I.mut, mut, N))) return st;
-  if (muEff != nullptr && (st = upload(I.mu, muEff, N))) return st;
+  CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
   return CFD_OK;
 }
 

@@ -145,6 +145,7 @@ class Solver {
   HostWallTable wall_;
   WallTable dWall_{};
   double* dStations_{nullptr};
+  double* dFaceStage_{nullptr};  // a face field in reference order, on its way in
   double* dForces_{nullptr};
 
   DeviceArena arena_;
