@@ -173,7 +173,16 @@ struct Engine {
   /// default shape.
   Status tunedShape(const Pending& q, const Solver& s, std::pair<int, int>* out) {
     if (!tuned) {
-      *out = {s.clusterSize(), s.threads()};
+      // By grid size as a lone solve runs, except that the mixed form takes
+      // clusters of at most 8 CTAs: its cost per iteration falls less than
+      // in proportion to the CTAs (the multigrid's coarse levels and its
+      // barriers do not shrink), so smaller clusters fit more solves per GPU
+      // (a 24-solve polar: 35 s on 8-CTA clusters, 37 s on 16, 43 s on 12),
+      // while the plain form needs 16 for its on-chip CG band (104 s on 16,
+      // 136 s on 12, 146 s on 8).
+      int R = s.clusterSize();
+      if (s.precision() == 1) R = std::min(R, 8);
+      *out = {R, s.threads()};
       return ok();
     }
     const auto key = std::make_tuple(s.cellsI(), s.cellsJ(), q.request.model, s.precision());

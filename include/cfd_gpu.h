@@ -308,8 +308,9 @@ cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued);
 /* Move up to `capacity` finished results into `out`; *count gets how many. */
 cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* count);
 /* Launch shapes of the solves the engine starts from now on: 0 (default) by
- * grid size, as a lone solve would run, which suits a few concurrent solves
- * (a polar); 1 tuned per grid for a saturated GPU (serving streams): the
+ * grid size, as a lone solve would run (the mixed form on clusters of at most
+ * 8 CTAs), which suits a few dozen concurrent solves (a polar); 1 tuned per
+ * grid for a saturated GPU (serving streams): the
  * cluster size with the most solve-iterations per second when as many solves
  * as fit run at once, measured once per grid and kept for the process. Either
  * way a grid always runs with the same shape, so results do not depend on
