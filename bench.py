@@ -494,6 +494,11 @@ def run_polar(args) -> None:
         engine.close()
         runs[form] = (results, cps)
         summary = _summarise(results, wall, cb)
+        if args.csv:
+            sweep = [r for r in results if reqs[r.id].designation.decode() == "2412"]
+            with open(f"{args.csv}_{form}.csv", "w") as fh:
+                fh.write(cb.polar_csv(sweep, [reqs[r.id].alpha_deg for r in sweep], "NACA 2412",
+                                      "768x192", 3e6, 1.0))
         summary["polar"] = [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
                              "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
                              "iterations": r.iterations, "ctas": r.cluster_size,
@@ -640,6 +645,9 @@ def main() -> None:
     ap.add_argument("--requests", type=int, default=512)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--csv", default="",
+                    help="polar: write the 2412 sweep of each form as <prefix>_<form>.csv "
+                         "in the reference's polar CSV layout")
     ap.add_argument("--graph", action="store_true",
                     help="c2: replay each step's launch from a CUDA graph")
     ap.add_argument("--form", choices=("plain", "mixed"), default="plain",

@@ -142,7 +142,8 @@ class Forces(C.Structure):
                 ("friction_drag_coefficient", C.c_double), ("lift", C.c_double),
                 ("drag", C.c_double), ("pitching_moment", C.c_double),
                 ("stagnation_chord_fraction", C.c_double), ("stations", C.c_int),
-                ("leading_edge", C.c_int)]
+                ("leading_edge", C.c_int), ("separation_upper_chord_fraction", C.c_double),
+                ("separation_lower_chord_fraction", C.c_double)]
 
 
 class CGridOptions(C.Structure):
@@ -554,7 +555,9 @@ class Result(C.Structure):
                 ("drag_coefficient", C.c_double), ("moment_coefficient", C.c_double),
                 ("pressure_drag_coefficient", C.c_double),
                 ("friction_drag_coefficient", C.c_double), ("submitted_s", C.c_double),
-                ("started_s", C.c_double), ("finished_s", C.c_double)]
+                ("started_s", C.c_double), ("finished_s", C.c_double),
+                ("separation_upper_chord_fraction", C.c_double),
+                ("separation_lower_chord_fraction", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -645,3 +648,39 @@ class Engine:
 def library_symbols() -> list[str]:
     """Names the C headers declare (for the ABI export check)."""
     return [name for name in dir(_lib) if name.startswith("cfd_")]
+
+
+# ---- polar CSV ------------------------------------------------------------------------
+def polar_csv(results, alphas, section: str, mesh: str, reynolds: float, speed: float,
+              chord: float = 1.0, moment_reference: float = 0.25,
+              continued_between_points: bool = False) -> str:
+    """A polar in the reference's CSV layout (post::toCsv, Polar.cpp:126-164),
+    so engine results can be diffed against the reference's examples/*.csv:
+    a commented header, then one row per solve in the order given. `results`
+    are engine Results, `alphas` their angles of attack in degrees. Separation
+    is an empty field where the surface stayed attached; l_over_d is 0 where
+    Cd is not positive (AerodynamicForces::liftToDrag, Forces.cpp:50-56)."""
+    lines = ["# cfd_simulator aerodynamic polar",
+             f"# section,{section or 'unknown'}",
+             f"# mesh,{mesh or 'unknown'}",
+             f"# reynolds,{reynolds:.6g}",
+             f"# freestream_speed_mps,{speed:.6g}",
+             f"# chord_m,{chord:.6g}",
+             f"# moment_reference_xc,{moment_reference:.6g}",
+             f"# continued_between_points,{'yes' if continued_between_points else 'no'}",
+             "# every row is a separate Navier-Stokes solve; nothing is interpolated",
+             "# status is converged, iteration-limit or diverged",
+             "alpha_deg,cl,cd,cd_pressure,cd_friction,cm,l_over_d,"
+             "separation_upper_xc,separation_lower_xc,status,iterations,continuity_residual"]
+    for r, alpha in zip(results, alphas):
+        cd = r.drag_coefficient
+        l_over_d = r.lift_coefficient / cd if (math.isfinite(cd) and cd > 0.0) else 0.0
+        upper = (f"{r.separation_upper_chord_fraction:.6f}"
+                 if r.separation_upper_chord_fraction >= 0.0 else "")
+        lower = (f"{r.separation_lower_chord_fraction:.6f}"
+                 if r.separation_lower_chord_fraction >= 0.0 else "")
+        lines.append(f"{alpha:.6f},{r.lift_coefficient:.8f},{cd:.8f},"
+                     f"{r.pressure_drag_coefficient:.8f},{r.friction_drag_coefficient:.8f},"
+                     f"{r.moment_coefficient:.8f},{l_over_d:.6f},{upper},{lower},"
+                     f"{STATUS_NAMES[r.status]},{r.iterations},{r.continuity:.6e}")
+    return "\n".join(lines) + "\n"

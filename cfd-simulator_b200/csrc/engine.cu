@@ -319,7 +319,9 @@ struct Engine {
     r.continuity = mon[kMonContinuity];
     r.momentum_x = mon[kMonMomX];
     r.momentum_y = mon[kMonMomY];
-    double f[10];
+    double f[12];
+    r.separation_upper_chord_fraction = -1.0;
+    r.separation_lower_chord_fraction = -1.0;
     std::vector<double> cp(static_cast<std::size_t>(std::max(s.solver->wallStations(), 1)));
     int stations = 0;
     if (status != CFD_SOLVE_DIVERGED &&
@@ -332,6 +334,8 @@ struct Engine {
       r.moment_coefficient = f[2];
       r.pressure_drag_coefficient = f[3];
       r.friction_drag_coefficient = f[4];
+      r.separation_upper_chord_fraction = f[10];
+      r.separation_lower_chord_fraction = f[11];
     }
     r.submitted_s = s.submitted;
     r.started_s = s.started;

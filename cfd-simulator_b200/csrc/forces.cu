@@ -136,6 +136,29 @@ __global__ void forcesKernel(WallTable w, const double* __restrict__ p, const do
   out[7] = moment;
   out[8] = (fp.chord > 0.0) ? w.cx[stag] / fp.chord : w.cx[stag];
   out[9] = static_cast<double>(stations);
+  // findSeparation (SurfaceData.cpp:179-203) on each surface, walked from the
+  // leading edge: the first pair of stations, neither of them the stagnation
+  // station, whose wall shear goes from positive to negative; the chordwise
+  // station is interpolated linearly between them. -1 where none is found.
+  for (int side = 0; side < 2; ++side) {
+    const int count = (side == 0) ? S - w.leadingEdge : w.leadingEdge;
+    double found = -1.0;
+    for (int m = 1; m < count; ++m) {
+      const int k = (side == 0) ? w.leadingEdge + m : w.leadingEdge - 1 - m;
+      const int kp = (side == 0) ? k - 1 : k + 1;  // the station before it
+      if (k == stag || kp == stag) continue;
+      const double before = station[static_cast<size_t>(kp) * kStationValues + 2];
+      const double after = station[static_cast<size_t>(k) * kStationValues + 2];
+      if (!(before > 0.0) || !(after < 0.0)) continue;
+      const double span = before - after;
+      const double fraction = (span > 0.0) ? before / span : 0.0;
+      const double xp = (fp.chord > 0.0) ? w.cx[kp] / fp.chord : w.cx[kp];
+      const double xk = (fp.chord > 0.0) ? w.cx[k] / fp.chord : w.cx[k];
+      found = xp + fraction * (xk - xp);
+      break;
+    }
+    out[10 + side] = found;
+  }
 }
 
 }  // namespace

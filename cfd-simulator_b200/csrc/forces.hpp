@@ -35,8 +35,9 @@ struct WallTable {
 /// coordinates; with none, the table stays empty).
 Status buildWallTable(const HostMesh& mesh, const double* nodes, HostWallTable* out);
 
-/// Launch the force integration; out gets 10 doubles (cfd_forces order:
-/// Cl, Cd, Cm, Cd_p, Cd_f, lift, drag, moment, stagnation x/c, stations).
+/// Launch the force integration; out gets 12 doubles (cfd_forces order:
+/// Cl, Cd, Cm, Cd_p, Cd_f, lift, drag, moment, stagnation x/c, stations,
+/// separation x/c on the upper and the lower surface or -1).
 Status launchForces(const WallTable& w, const double* p, const double* u, const double* v,
                     const double* mu, double dynamicPressure, double referencePressure,
                     double chord, double cosA, double sinA, double* station, double* out,

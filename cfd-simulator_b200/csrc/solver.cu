@@ -941,9 +941,9 @@ Status Solver::forces(double speed, double alphaDeg, double density, double refe
     return st;
   }
   CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
-  double h[10];
+  double h[12];
   CUDA_OR_FAIL(cudaMemcpy(h, dForces_, sizeof(h), cudaMemcpyDeviceToHost));
-  std::copy(h, h + 10, out);
+  std::copy(h, h + 12, out);
   const int S = wall_.count();
   if (stations != nullptr) *stations = S;
   if (leadingEdge != nullptr) *leadingEdge = wall_.leadingEdge;
@@ -1138,7 +1138,7 @@ cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double d
                           double* cf) {
   if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
   if (out == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null output");
-  double v[10];
+  double v[12];
   int stations = 0, leadingEdge = 0;
   if (cfd_status st = h->solver->forces(speed, alpha_deg, density, reference_pressure, chord, v, cp, cf,
                                         &stations, &leadingEdge);
@@ -1156,6 +1156,8 @@ cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double d
   out->stagnation_chord_fraction = v[8];
   out->stations = static_cast<int>(v[9]);
   out->leading_edge = leadingEdge;
+  out->separation_upper_chord_fraction = v[10];
+  out->separation_lower_chord_fraction = v[11];
   (void)stations;
   return CFD_OK;
 }

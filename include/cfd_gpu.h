@@ -182,6 +182,9 @@ typedef struct cfd_forces {
   double stagnation_chord_fraction;
   int stations;     /* wall stations: upper (leading edge -> trailing edge) then lower */
   int leading_edge; /* number of lower-surface stations */
+  /* findSeparation (SurfaceData.cpp:179-203): x/c where the wall shear first
+   * turns negative walking away from the leading edge, or -1 */
+  double separation_upper_chord_fraction, separation_lower_chord_fraction;
 } cfd_forces;
 
 /* speed, alpha_deg, density and reference_pressure describe the freestream
@@ -294,6 +297,7 @@ typedef struct cfd_result {
   double lift_coefficient, drag_coefficient, moment_coefficient;
   double pressure_drag_coefficient, friction_drag_coefficient;
   double submitted_s, started_s, finished_s;  /* engine clock, seconds */
+  double separation_upper_chord_fraction, separation_lower_chord_fraction;  /* or -1 */
 } cfd_result;
 
 /* memory_budget_bytes: device memory the resident solves may hold (0: 80 %

@@ -582,7 +582,8 @@ void ref_green_gauss(void* m, const double* faceValues, double* out) {
 
 /// extractSurface + integrateForces on the solver's current field
 /// (SurfaceData.cpp:208-348, Forces.cpp:60-130). out = {Cl, Cd, Cm, Cd_p,
-/// Cd_f, stations}; cp, if not null, receives Cp for upper then lower stations.
+/// Cd_f, stations, upper and lower separation x/c or -1}; cp, if not null,
+/// receives Cp for upper then lower stations.
 int ref_forces(void* s, double speed, double alphaDeg, double density, double reynolds,
                double chord, double* out, double* cp) {
   RefSolver* r = static_cast<RefSolver*>(s);
@@ -608,6 +609,9 @@ int ref_forces(void* s, double speed, double alphaDeg, double density, double re
   out[3] = fv.pressureDragCoefficient;
   out[4] = fv.frictionDragCoefficient;
   out[5] = static_cast<double>(fv.stations);
+  const auto& sd = surface.value();
+  out[6] = sd.upperSeparation.found ? sd.upperSeparation.chordFraction : -1.0;
+  out[7] = sd.lowerSeparation.found ? sd.lowerSeparation.chordFraction : -1.0;
   if (cp != nullptr) {
     std::size_t k = 0;
     for (const auto& point : surface.value().upper) cp[k++] = point.pressureCoefficient;

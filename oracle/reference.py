@@ -215,7 +215,8 @@ class RefSolver:
         return out
 
     def forces(self, speed, alpha_deg, density, reynolds, chord=1.0):
-        out = np.zeros(6)
+        """(Cl, Cd, Cm, Cd_p, Cd_f, stations, upper and lower separation x/c or -1), Cp."""
+        out = np.zeros(8)
         cp = np.zeros(4 * self.mesh.faces)
         if lib().ref_forces(self._h, speed, alpha_deg, density, reynolds, chord, _p(out), _p(cp)) != 0:
             raise ValueError(lib().ref_last_error().decode())

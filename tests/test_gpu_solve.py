@@ -146,3 +146,31 @@ def test_converged_forces_match_the_reference(name):
     assert f.drag_coefficient == pytest.approx(ref[1], rel=1e-7)
     assert f.moment_coefficient == pytest.approx(ref[2], rel=1e-7)
     assert np.max(np.abs(cp - g["converged/cp"])) < 1e-7
+
+
+SEPARATION = ["laminar_a10", "laminar_a16", "sst_2412_a14"]
+
+
+@pytest.mark.parametrize("name", SEPARATION)
+def test_separation_points_match_the_reference(name):
+    """findSeparation on the device (upper and lower surface, -1 where the
+    layer stays attached) on the reference's own field at an incidence where
+    it separates, with Cl/Cd/Cm and Cp as extractSurface/integrateForces give
+    them (golden vectors from tests/golden/make_separation.py)."""
+    g = golden("separation")
+    sp, wp, npn, fl = g[f"{name}/grid"]
+    des, alpha = str(g[f"{name}/designation"]), float(g[f"{name}/alpha"])
+    mesh = cb.cgrid(des, surface_points=int(sp), wake_points=int(wp), normal_points=int(npn),
+                    first_layer_height=float(fl), upstream_chords=10.0, downstream_chords=15.0,
+                    vertical_chords=10.0)
+    d = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), cb.Settings.defaults())
+    d.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, 1e6))
+    d.load_state(u=g[f"{name}/u"], v=g[f"{name}/v"], p=g[f"{name}/p"], mu_eff=g[f"{name}/mu_eff"])
+    f, cp, _ = d.forces(1.0, alpha, 1.0)
+    ref = g[f"{name}/forces"]
+    assert f.lift_coefficient == pytest.approx(ref[0], rel=1e-12)
+    assert f.drag_coefficient == pytest.approx(ref[1], rel=1e-12)
+    assert f.moment_coefficient == pytest.approx(ref[2], rel=1e-12, abs=1e-15)
+    assert np.max(np.abs(cp - g[f"{name}/cp"])) <= 1e-12 * max(1.0, np.max(np.abs(cp)))
+    assert f.separation_upper_chord_fraction == pytest.approx(ref[6], abs=1e-12)
+    assert f.separation_lower_chord_fraction == pytest.approx(ref[7], abs=1e-12)
