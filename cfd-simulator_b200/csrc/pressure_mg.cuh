@@ -81,26 +81,6 @@ DEV void forCells(const Lv& L, const Span& s, F&& f) {
   }
 }
 
-/// f(c, i, j) for the cells of one colour ((i + j) & 1) of the span; with
-/// NI even every row holds NI / 2 of them.
-template <typename F>
-DEV void forColour(const Lv& L, const Span& s, int colour, F&& f) {
-  if ((L.NI & 1) == 0) {
-    const int half = L.NI >> 1;
-    const int count = (s.j1 - s.j0) * half;
-    for (int m = s.tid; m < count; m += s.T) {
-      const int jj = m / half;
-      const int j = s.j0 + jj;
-      const int i = 2 * (m - jj * half) + ((colour + j) & 1);
-      f(j * L.NI + i, i, j);
-    }
-  } else {
-    forCells(L, s, [&](int c, int i, int j) {
-      if (((i + j) & 1) == colour) f(c, i, j);
-    });
-  }
-}
-
 /// Neighbour indices of cell (i, j) for branch-free row products: a missing
 /// neighbour is replaced by the cell itself, whose coefficient on that side
 /// is zero on every level (the fine rows are built that way and the Galerkin
