@@ -60,8 +60,9 @@ constexpr double kSigmaK1 = 0.85, kSigmaW1 = 0.5, kBeta1 = 0.075;
 constexpr double kSigmaK2 = 1.0, kSigmaW2 = 0.856, kBeta2 = 0.0828;
 constexpr double kBetaStar = 0.09, kKappa = 0.41, kA1 = 0.31, kProdLimit = 10.0;
 
-// BoundaryKind values (cfd_gpu.h).
-constexpr int kInternal = 0, kInlet = 1, kOutlet = 2, kFarField = 3, kWall = 4;
+// BoundaryKind values the kernel tests for (cfd_gpu.h CFD_BC_*; outlet and
+// internal faces need no test of their own).
+constexpr int kInlet = CFD_BC_INLET, kFarField = CFD_BC_FARFIELD, kWall = CFD_BC_NOSLIP_WALL;
 
 // ---- faces of a cell ----------------------------------------------------------
 
