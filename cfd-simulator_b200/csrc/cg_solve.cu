@@ -36,7 +36,7 @@ struct CgView {
   double *x, *r, *z, *q, *d0, *d1;
   int maxIt;
   double tol;
-  double* report;  // {iterations, initial, final, converged}
+  double* report;  // {iterations, initial, final, converged, bad wake map}: 8 words
 };
 
 namespace {
@@ -146,17 +146,28 @@ __global__ void __launch_bounds__(512, 1) cgSolveKernel(CgView V) {
   t.T = blockDim.x;
   t.c0 = static_cast<int>((static_cast<long long>(V.N) * t.rank) / t.R);
   t.c1 = static_cast<int>((static_cast<long long>(V.N) * (t.rank + 1)) / t.R);
+  if (V.report[4] != 0.0) return;  // a bad wake map (every CTA sees the same flag)
   cgSolveTeam(V, t, sh);
   t.cl.sync();  // no CTA leaves while a peer may still read its shared memory
 }
 
 /// Reference-order face coefficients -> device layout; missing wake map -> -1.
+/// A wake-map entry that names no cell of the block (>= cells) would make the
+/// solve read outside x: it is replaced by -1 and flagged in report[4], and the
+/// solve kernel then leaves x untouched.
 __global__ void cgLayoutKernel(int NI, int NJ, const double* upper, const int* across, double* pN,
-                               double* pE, int* acrossOut) {
+                               double* pE, int* acrossOut, double* report) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   const int jFaces = NI * (NJ + 1);
   const int faces = jFaces + (NI + 1) * NJ;
-  if (f < NI) acrossOut[f] = (across != nullptr) ? across[f] : -1;
+  if (f < NI) {
+    int a = (across != nullptr) ? across[f] : -1;
+    if (a >= NI * NJ) {
+      report[4] = 1.0;
+      a = -1;
+    }
+    acrossOut[f] = (a >= 0) ? a : -1;
+  }
   if (f >= faces) return;
   if (f < jFaces) {
     pN[f] = upper[f];
@@ -186,16 +197,21 @@ Status cgCheck(const cfd_cg_system* s, const double* x, int maxIt, CgView* V) {
 Status cgRun(const cfd_cg_system* s, CgView V, cudaStream_t stream) {
   const int faces = V.NI * (V.NJ + 1) + (V.NI + 1) * V.NJ;
   const int block = 256;
+  cudaError_t e = cudaMemsetAsync(V.report + 4, 0, sizeof(double), stream);
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
   cgLayoutKernel<<<(faces + block - 1) / block, block, 0, stream>>>(
       V.NI, V.NJ, s->upper, s->across_j0, const_cast<double*>(V.pN), const_cast<double*>(V.pE),
-      const_cast<int*>(V.acrossJ0));
-  cudaError_t e = cudaGetLastError();
+      const_cast<int*>(V.acrossJ0), V.report);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-  static bool configured = false;
-  if (!configured) {
-    e = cudaFuncSetAttribute(cgSolveKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-    configured = true;
+  // the non-portable cluster size is a per-device kernel attribute
+  static PerDeviceOnce configured;
+  if (Status st = configured.run([]() -> Status {
+        const cudaError_t a = cudaFuncSetAttribute(cgSolveKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        return (a == cudaSuccess) ? ok() : fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(a));
+      });
+      st != CFD_OK) {
+    return st;
   }
   const int R = chooseClusterSize(V.N);
   cudaLaunchConfig_t config = {};
@@ -214,6 +230,21 @@ Status cgRun(const cfd_cg_system* s, CgView V, cudaStream_t stream) {
   return CFD_OK;
 }
 
+/// Wait for the solve on `stream`, then copy its report to the host (4
+/// doubles, may be null); a wake map that names a cell outside the block is
+/// an invalid argument (the solve did not run).
+Status cgReport(const CgView& V, cudaStream_t stream, double* report) {
+  double host[5];
+  cudaError_t e = cudaMemcpyAsync(host, V.report, sizeof(host), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  if (host[4] != 0.0) {
+    return fail(CFD_INVALID_ARGUMENT, "across_j0 names a cell outside the block (entries must be < cells_i*cells_j)");
+  }
+  if (report != nullptr) for (int k = 0; k < 4; ++k) report[k] = host[k];
+  return CFD_OK;
+}
+
 }  // namespace cfdb
 
 extern "C" {
@@ -226,8 +257,8 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   const std::size_t FN = static_cast<std::size_t>(V.NI) * (V.NJ + 1);
   const std::size_t FE = static_cast<std::size_t>(V.NI + 1) * V.NJ;
   // Scratch for this call: both coefficient families, five CG vectors, the
-  // wake map and the report.
-  const std::size_t doubles = FN + FE + 5 * N + 4;
+  // report (8 words) and the wake map.
+  const std::size_t doubles = FN + FE + 5 * N + 8;
   char* scratch = nullptr;
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&scratch), doubles * sizeof(double) + V.NI * sizeof(int));
   if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
@@ -239,7 +270,7 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   V.q = p; p += N;
   V.d0 = p; p += N;
   V.d1 = p; p += N;
-  V.report = p; p += 4;
+  V.report = p; p += 8;
   V.acrossJ0 = reinterpret_cast<const int*>(p);
   V.diag = system->diag;
   V.b = system->source;
@@ -248,13 +279,7 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   V.tol = tolerance;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cfd_status st = cfdb::cgRun(system, V, s);
-  if (st == CFD_OK) {
-    double host[4];
-    e = cudaMemcpyAsync(host, V.report, sizeof(host), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) st = cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-    else if (report != nullptr) for (int k = 0; k < 4; ++k) report[k] = host[k];
-  }
+  if (st == CFD_OK) st = cfdb::cgReport(V, s, report);
   cudaFree(scratch);
   return st;
 }
@@ -286,16 +311,20 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
 //     caller.
 //   * the first call on each device resolves the array's device address with
 //     cudaGetSymbolAddress, with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture begins. Every call waits for its solve to
+//     finish on its stream before returning.
+//   * a wake-map entry that names no cell of the block is refused with
+//     CFD_INVALID_ARGUMENT (the solve does not run; x is left as it was).
 
 namespace cfdb {
 namespace {
 
 constexpr long long kNoAllocMaxNodes = 65536;
 // 7 arrays of at most kNoAllocMaxNodes doubles (two face families and five
-// cell vectors, each at most (cells_i+1)*(cells_j+1) long), 4 report words,
-// and the wake map (cells_i ints) in the last kNoAllocMaxNodes/2 doubles.
-constexpr std::size_t kNoAllocDoubles = 7 * kNoAllocMaxNodes + 4 + kNoAllocMaxNodes / 2;
+// cell vectors, each at most (cells_i+1)*(cells_j+1) long), 8 report words,
+// and the wake map (cells_i <= 32,767 ints) in the last kNoAllocMaxNodes/2
+// doubles.
+constexpr std::size_t kNoAllocDoubles = 7 * kNoAllocMaxNodes + 8 + kNoAllocMaxNodes / 2;
 
 static __device__ __align__(256) double g_noAllocScratch[kNoAllocDoubles];
 
@@ -349,7 +378,7 @@ cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double t
   V.d0 = base + 5 * slot;
   V.d1 = base + 6 * slot;
   V.report = base + 7 * slot;
-  V.acrossJ0 = reinterpret_cast<const int*>(base + 7 * slot + 4);
+  V.acrossJ0 = reinterpret_cast<const int*>(base + 7 * slot + 8);
   V.diag = system->diag;
   V.b = system->source;
   V.x = x;
@@ -357,12 +386,7 @@ cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double t
   V.tol = tolerance;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (cfd_status st = cfdb::cgRun(system, V, s); st != CFD_OK) return st;
-  double host[4];
-  cudaError_t e = cudaMemcpyAsync(host, V.report, sizeof(host), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-  if (report != nullptr) for (int k = 0; k < 4; ++k) report[k] = host[k];
-  return CFD_OK;
+  return cfdb::cgReport(V, s, report);
 }
 
 }  // extern "C"

@@ -1524,17 +1524,20 @@ int cgSharedBytes(int NI, int NJ, int clusterSize) {
 
 namespace {
 
+PerDeviceOnce g_simpleKernelConfigured;
+
+/// The non-portable cluster size (16) and the dynamic shared-memory limit
+/// are attributes of the kernel on each device: set them on every device
+/// this process launches on.
 Status configureSimpleKernel() {
-  static bool configured = false;
-  if (!configured) {
+  return g_simpleKernelConfigured.run([]() -> Status {
     cudaError_t e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     if (e == cudaSuccess) {
       e = cudaFuncSetAttribute(simpleKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxCgSharedBytes);
     }
     if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-    configured = true;
-  }
-  return ok();
+    return ok();
+  });
 }
 
 }  // namespace

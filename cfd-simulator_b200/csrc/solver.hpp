@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.hpp"
@@ -18,6 +19,31 @@
 #include "instance.hpp"
 
 namespace cfdb {
+
+/// Set-up that must happen once on every CUDA device a process uses (kernel
+/// attributes such as the dynamic shared-memory limit are per device), from
+/// any host thread. run() calls `setup` with the device current the first
+/// time it sees that device, under a lock, and remembers success.
+class PerDeviceOnce {
+ public:
+  template <typename F>
+  Status run(F&& setup) {
+    int device = 0;
+    const cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    if (device < 0 || device >= kMaxDevices) return fail(CFD_OUT_OF_RANGE, "device ordinal too large");
+    std::lock_guard<std::mutex> lock(mutex_);
+    if (done_[device]) return CFD_OK;
+    const Status st = setup();
+    if (st == CFD_OK) done_[device] = true;
+    return st;
+  }
+
+ private:
+  static constexpr int kMaxDevices = 64;
+  std::mutex mutex_;
+  bool done_[kMaxDevices] = {};
+};
 
 /// One cudaMalloc carved into aligned arrays; released as a whole.
 class DeviceArena {

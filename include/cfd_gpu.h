@@ -241,7 +241,8 @@ typedef struct cfd_cg_system {
  * final residual, converged}; both residuals are L1 norms as in the
  * reference. Allocates its scratch (two coefficient arrays, five vectors) for
  * the call. stream: a cudaStream_t, or NULL for the legacy default stream.
- * Returns after the solve has finished. */
+ * Returns after the solve has finished. A wake-map entry >= cells_i*cells_j
+ * is refused with CFD_INVALID_ARGUMENT, and x is then left unchanged. */
 cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance,
                         int max_iterations, double* report, void* stream);
 
@@ -254,8 +255,10 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
  * (cells_i+1)*(cells_j+1) <= 65536 nodes; larger ones return
  * CFD_OUT_OF_RANGE. All calls on a device share that array; calls that
  * overlap on the GPU race and must be serialised by the caller. The first call
- * on each device resolves the array's address; make it before any stream
- * capture. Results equal cfd_cg_solve's. */
+ * on each device resolves the array's address (cudaGetSymbolAddress, with
+ * that device current); make that first call before any stream capture
+ * begins. Like cfd_cg_solve, every call returns after its solve has finished.
+ * Results equal cfd_cg_solve's. */
 cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double tolerance,
                                 int max_iterations, double* report, void* stream);
 

@@ -21,6 +21,8 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
     for target in (os.path.join(ROOT, "oracle"), PKG):
         subprocess.run(["make", "-s", "-C", target], check=True)
+    # the reference-side binding's driver (a message only where the reference is absent)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "shim"], check=True)
 
 
 def _has_gpu() -> bool:

@@ -64,6 +64,57 @@ class Case:
         return s
 
 
+def digest(a: np.ndarray) -> str:
+    """SHA-256 of an array's values as little-endian float64 (int32 for index
+    arrays): the form tests/golden/make_baseline_golden.py stores."""
+    import hashlib
+    a = np.asarray(a)
+    a = np.ascontiguousarray(a, "<i4" if a.dtype.kind in "iu" else "<f8")
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+class BaselineCase:
+    """A benchmark-size case (c1 192x48 laminar, c2 384x96 SST, c3 768x192
+    SST) from tests/golden/baseline_sizes.npz, meshed by the library's own
+    generator (pinned bit for bit to the reference's at these sizes)."""
+
+    _golden = None
+
+    def __init__(self, name: str):
+        if BaselineCase._golden is None:
+            BaselineCase._golden = golden("baseline_sizes")
+        g = BaselineCase._golden
+        self.name = name
+        self.g = {k.split("/", 1)[1]: v for k, v in g.items() if k.startswith(name + "/")}
+        sp, wp, npn, fl = self.g["grid"]
+        self.designation = str(self.g["designation"])
+        self.mesh = cb.cgrid(self.designation, surface_points=int(sp), wake_points=int(wp),
+                             normal_points=int(npn), first_layer_height=float(fl),
+                             upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0)
+        self.model = int(self.g["model"])
+        self.alpha = float(self.g["alpha"])
+        self.reynolds = float(self.g["reynolds"])
+        self.packed = self.g["settings"]
+        self.conditions = cb.freestream_conditions(self.mesh, 1.0, self.alpha)
+        self.initial = cb.uniform_field(self.mesh, 1.0, self.alpha, 1.0, self.reynolds)
+
+    def settings(self, precision: int = 0) -> cb.Settings:
+        p = self.packed
+        return cb.Settings.defaults(precision=precision, inflow_intensity=p[7],
+                                    inflow_viscosity_ratio=p[8])
+
+    def oracle(self, gs_order=port.DEVICE_ORDER) -> port.OracleSolver:
+        s = port.OracleSolver(self.mesh, self.conditions, self.packed, self.model, gs_order)
+        s.initialise(*self.initial)
+        return s
+
+    def device(self, precision: int = 0) -> "cb.SimpleSolver":
+        s = cb.SimpleSolver.create(self.mesh, self.conditions, self.settings(precision))
+        s.set_turbulence_model(self.model)
+        s.initialise(*self.initial)
+        return s
+
+
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     """max |a - b| / max(max |b|, tiny): an infinity-norm relative error."""
     scale = max(float(np.max(np.abs(b))), 1e-300)

@@ -1,0 +1,183 @@
+"""Device parity at the benchmark grid sizes, through the C ABI: 192x48
+laminar (c1), 384x96 SST (c2) and 768x192 SST (c3), the grids of the
+single-solve benchmark configurations and of the batched polar.
+
+These sizes take launch paths the small golden cases never reach: clusters
+of 8 and 16 CTAs with DSMEM halos between row bands, the k/omega sweeps
+pipelined over six CTAs, the pressure CG from global memory (768x192, or any
+size with CFD_KERNEL_FLAGS=1) and, in the mixed form, multigrid levels split
+over the cluster in global memory. Each is compared with the CPU oracle, which
+test_oracle_baseline_sizes.py pins bit for bit to the reference at the same
+sizes; the c1 solve also with the reference's own converged answer.
+
+Tolerances: the stages before the pressure CG are bit-identical (no
+reduction); the CG's dot products sum in a different order, so fields after
+it agree to 1e-9 relative after one iteration and 1e-7 after twenty (the
+same bounds as the small cases); converged fields 1e-9 relative L2 and
+Cl/Cd/Cm 1e-7 relative, the parity contract."""
+import numpy as np
+import pytest
+
+import cfd_b200 as cb
+from helpers import BaselineCase, rel_err, rel_l2
+from oracle import port
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["c1", "c2", "c3"]
+FIELDS = {"U": 0, "V": 1, "P": 2, "MASS_FLUX": 5, "K": 22, "OMEGA": 23, "MUT": 24}
+PRE_CG = [("GRADIENTS", ["GRAD_U", "GRAD_V", "GRAD_P"]),
+          ("MOMENTUM_ASSEMBLY", ["MOM_DIAG", "MOM_SOURCE_U", "MOM_SOURCE_V", "MOM_UPPER"]),
+          ("MOMENTUM_SOLVE", ["U", "V"]),
+          ("RHIE_CHOW", ["MASS_FLUX"]),
+          ("PRESSURE_ASSEMBLY", ["P_DIAG", "P_SOURCE", "P_UPPER", "NET_FLUX"])]
+# kernel flag bit 0: the pressure CG runs from global memory even where its
+# band fits in shared memory; the two loops must give the same answers
+KERNEL_FLAGS = [0, 1]
+_CASES: dict = {}
+_TWENTY: dict = {}
+
+
+def _case(name):
+    if name not in _CASES:
+        _CASES[name] = BaselineCase(name)
+    return _CASES[name]
+
+
+def _oracle_twenty(c):
+    """Monitors and fields of the oracle (device sweep order) after 20
+    iterations; computed once per case (768x192 takes ~15 s on one core)."""
+    if c.name not in _TWENTY:
+        o = c.oracle(port.DEVICE_ORDER)
+        mon = o.iterate(20)
+        _TWENTY[c.name] = (mon, {k: o.read(f) for k, f in FIELDS.items()})
+    return _TWENTY[c.name]
+
+
+def _fields(c):
+    return [f for f in FIELDS if c.model == 2 or f not in ("K", "OMEGA", "MUT")]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_stages_before_the_pressure_solve_are_bit_identical(name):
+    c = _case(name)
+    for stage, fields in PRE_CG:
+        o = c.oracle(port.DEVICE_ORDER)
+        o.iterate(1, stop_stage=cb.STAGE[stage])
+        d = c.device()
+        d.iterate_partial(stage)
+        for field in fields:
+            a, b = d.read(field), o.read(cb.FIELD[field])
+            assert np.array_equal(a, b), f"{stage}/{field}: rel err {rel_err(a, b):.3e}"
+        d.close()
+
+
+@pytest.mark.parametrize("flags", KERNEL_FLAGS)
+@pytest.mark.parametrize("name", CASES)
+def test_first_iteration_after_the_pressure_solve(name, flags, monkeypatch):
+    monkeypatch.setenv("CFD_KERNEL_FLAGS", str(flags))
+    c = _case(name)
+    o = c.oracle(port.DEVICE_ORDER)
+    mo = o.iterate(1)
+    d = c.device()
+    mon = d.iterate(1)
+    assert abs(mon.pressure_iterations - mo[0, 5]) <= 1
+    assert mon.continuity == pytest.approx(mo[0, 0], rel=1e-12)
+    for field in _fields(c):
+        a, b = d.read(field), o.read(FIELDS[field])
+        assert rel_err(a, b) < 1e-9, (field, rel_err(a, b))
+
+
+@pytest.mark.parametrize("flags", KERNEL_FLAGS)
+@pytest.mark.parametrize("name", CASES)
+def test_twenty_iterations_track_the_oracle(name, flags, monkeypatch):
+    monkeypatch.setenv("CFD_KERNEL_FLAGS", str(flags))
+    c = _case(name)
+    mo, fo = _oracle_twenty(c)
+    d = c.device()
+    _, hist = d.iterate(20, history=True)
+    assert np.all(np.isfinite(hist))
+    assert np.max(np.abs(hist[:, 5] - mo[:, 5])) <= 1
+    for k in (0, 1, 2):  # continuity, momentum x, momentum y
+        assert np.max(np.abs(hist[:, k] - mo[:, k]) / np.abs(mo[:, k])) < 1e-7, k
+    for field in _fields(c):
+        err = rel_err(d.read(field), fo[field])
+        assert err < 1e-7, (field, err)
+
+
+def test_c1_on_sixteen_ctas_tracks_the_oracle(monkeypatch):
+    """192x48 on the 16-CTA clusters it runs on when batched with the larger
+    grids of the polar (three rows per CTA)."""
+    monkeypatch.setenv("CFD_CLUSTER_SIZE", "16")
+    c = _case("c1")
+    mo, fo = _oracle_twenty(c)
+    d = c.device()
+    shape = cb.Batch([d])
+    assert shape.shape()[0] == 16
+    shape.close()
+    _, hist = d.iterate(20, history=True)
+    assert np.max(np.abs(hist[:, 5] - mo[:, 5])) <= 1
+    for field in _fields(c):
+        assert rel_err(d.read(field), fo[field]) < 1e-7, field
+
+
+def test_c1_converged_matches_the_reference():
+    """192x48 laminar, alpha 0, Re 500, converged (worst residual < 1e-12,
+    then 2000 settling iterations, as the reference's golden was made):
+    u, v, p within 1e-9 relative L2 and Cl, Cd, Cm within 1e-7 of the
+    reference's (Cl and Cm vanish at alpha 0 on the symmetric section, so
+    they are compared in absolute terms against Cd's scale)."""
+    c = _case("c1")
+    g = c.g
+    d = c.device()
+    taken, mon = d.converge(200000, 1e-12)
+    assert mon.worst() < 1e-12, (taken, mon.worst())
+    d.iterate(2000)
+    for field, key in (("U", "u"), ("V", "v"), ("P", "p")):
+        err = rel_l2(d.read(field), g[f"converged/{key}"])
+        assert err < 1e-9, (field, err)
+    f, cp, _ = d.forces(1.0, c.alpha, 1.0)
+    ref = g["converged/forces"]
+    scale = abs(ref[1])
+    assert f.drag_coefficient == pytest.approx(ref[1], rel=1e-7)
+    assert abs(f.lift_coefficient - ref[0]) <= 1e-7 * scale
+    assert abs(f.moment_coefficient - ref[2]) <= 1e-7 * scale
+    assert np.max(np.abs(cp - g["converged/cp"])) < 1e-7
+
+
+def _l1_residual(c, d):
+    diag, source, upper = d.read("P_DIAG"), d.read("P_SOURCE"), d.read("P_UPPER")
+    y = port.ldu_multiply(c.mesh, diag, upper, upper, d.read("P_CORRECTION"))
+    return float(np.sum(np.abs(source - y))), float(np.sum(np.abs(source)))
+
+
+@pytest.mark.parametrize("warm", [0, 5])
+@pytest.mark.parametrize("name", ["c2", "c3"])
+def test_mixed_pressure_solve_meets_the_stopping_rule(name, warm):
+    """The mixed form's FP32 multigrid CG inside FP64 refinement, with its
+    finest levels split over the cluster in global memory (36,864 and 9,216
+    cells at 384x96; 147,456, 36,864 and 9,216 at 768x192), meets the
+    reference's rule sum |b - A x| <= 0.01 sum |b| on the FP64 system."""
+    c = _case(name)
+    s = c.settings(precision=1)
+    s.inner_iterations = 0  # up to pressure_iterations, so the rule decides
+    d = cb.SimpleSolver.create(c.mesh, c.conditions, s)
+    d.set_turbulence_model(c.model)
+    d.initialise(*c.initial)
+    if warm:
+        d.iterate(warm)
+    mon = d.iterate_partial("PRESSURE_SOLVE")
+    res, b = _l1_residual(c, d)
+    assert 0 < mon.pressure_iterations < 200
+    assert res <= 0.01 * b * (1 + 1e-9), (res / b, mon.pressure_iterations)
+
+
+@pytest.mark.parametrize("name", ["c2", "c3"])
+def test_mixed_assembly_is_the_fp64_assembly(name):
+    c = _case(name)
+    o = c.oracle(port.DEVICE_ORDER)
+    o.iterate(1, stop_stage=cb.STAGE["MOMENTUM_ASSEMBLY"])
+    d = c.device(precision=1)
+    d.iterate_partial("MOMENTUM_ASSEMBLY")
+    for field in ("MOM_DIAG", "MOM_SOURCE_U", "MOM_SOURCE_V", "MOM_UPPER"):
+        assert np.array_equal(d.read(field), o.read(cb.FIELD[field])), field
