@@ -1,24 +1,32 @@
-"""Benchmark: steady SIMPLE (k-omega SST, plain FP64) on NACA 0012 C-grids.
+"""Benchmark: the batched polar of steady SIMPLE solves (k-omega SST, plain FP64).
 
-Workload (one "step" = one SIMPLE outer iteration of every solve in it):
-  NACA 0012, Re 1e6, k-omega SST, inflow intensity 0.1 %, mu_t/mu 10,
-  medium C-grid 384 x 96 cells (surface 128, wake 65, normal 97 points;
-  upstream/vertical 10 chords, downstream 15; first layer 1e-5 chord),
-  two solves at alpha 0 deg and 4 deg in one batched launch. Synthetic inputs:
+Workload (one "step" = one SIMPLE outer iteration of every solve in it, all
+in one batched launch, one thread-block cluster per solve):
+  a 21-point NACA 2412 polar, Re 3e6, alpha -4..16 deg step 1, on the fine
+  C-grid 768 x 192 cells (surface 256, wake 129, normal 193 points; first
+  layer 5e-6 chord), plus NACA 0012 at Re 1e6, alpha 4 deg, on the coarse
+  192 x 48 (first layer 2e-3), medium 384 x 96 (1e-5) and fine 768 x 192
+  (5e-6) C-grids: 24 solves of uneven size, 3,290,112 cells resident at once
+  (3.2 GB of device state). k-omega SST, inflow intensity 0.1 %, mu_t/mu 10;
+  domains 10 chords upstream and vertically, 15 downstream. Synthetic inputs:
   the uniform freestream start of FlowField::uniform, advanced by the warm-up
   steps; no dataset exists for this path.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line (rank 0). `value` is cell-iterations/s over all ranks,
-timed with CUDA events around each step's launch on the launching stream; L2
-(126 MB) is flushed between timed steps by writing a 256 MiB buffer. `e2e` is
-the same metric through the C ABI from pinned host buffers: each step loads
-the solver state host->device, iterates once, and reads the monitors back.
-`--impl reference` times the reference's own CPU solver (compiled from its
-sources into oracle/_ref) on the same workload with every host core.
-Multi-GPU (torchrun): independent replicas, one per GPU; no collective on the
-data path (weak scaling).
+Prints one JSON line (rank 0). `value` is cell-iterations/s of the plain FP64
+form over all ranks, timed with CUDA events around each step's launch on the
+launching stream; the state (3.2 GB) is larger than the L2 (126 MB), and a
+256 MiB buffer is written between timed steps besides. `e2e` is the same
+metric through the C ABI from pinned host buffers: every step loads each
+solve's state host->device, iterates the batch once and reads each solve's
+u, v and p back. The same line carries the mixed FP32/FP64 form's figures on
+the same workload, both forms' polar solved to convergence (solves/min,
+time-to-convergence percentiles, per-point Cl/Cd/Cm/Cp differences) and the
+reference's CPU solver timed on the host's cores. `--impl reference` times the
+reference's own CPU solver (compiled from its sources into oracle/_ref) on the
+same workload with the host's cores. Multi-GPU (torchrun): independent
+replicas, one per GPU; no collective on the data path (weak scaling).
 """
 from __future__ import annotations
 
@@ -41,24 +49,41 @@ for _p in (ROOT, PKG):
 
 METRIC = "SIMPLE cell-iters/s, % HBM roofline; solves/min + p99, mixed vs FP64 at ΔCl≤1e-4"
 UNIT = "cell-iters/s"
-WORKLOAD = dict(designation="0012", surface_points=128, wake_points=65, normal_points=97,
-                first_layer_height=1e-5, upstream_chords=10.0, downstream_chords=15.0,
-                vertical_chords=10.0)
-ALPHAS = (0.0, 4.0)
 REYNOLDS = 1e6
 INTENSITY = 0.001
 VISCOSITY_RATIO = 10.0
+EXTENTS = dict(upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0)
+GRIDS = {  # (surface, wake, normal) points; cells 192x48, 384x96, 768x192
+    "coarse": (64, 33, 49), "medium": (128, 65, 97), "fine": (256, 129, 193),
+}
+# The batched polar: (designation, alpha, Reynolds, grid, first layer height)
+POLAR = ([("2412", float(a), 3e6, "fine", 5e-6) for a in range(-4, 17)]
+         + [("0012", 4.0, 1e6, "coarse", 2e-3), ("0012", 4.0, 1e6, "medium", 1e-5),
+            ("0012", 4.0, 1e6, "fine", 5e-6)])
+POLAR_NAME = ("batched polar: NACA2412 k-omega SST Re3e6 C-grid 768x192, alpha -4..16 step 1 "
+              "(21 solves) + NACA0012 k-omega SST Re1e6 alpha 4 on 192x48/384x96/768x192, "
+              "24 solves in one launch")
+# The mixed form runs on clusters of at most 8 CTAs (the engine's default
+# policy for it: smaller clusters fit more of its solves on the GPU).
+MIXED_CLUSTER = 8
+# The former headline pair (384 x 96, alpha 0 and 4), kept as --workload c2.
+C2_ALPHAS = (0.0, 4.0)
 
 
-def config(extra=None):
-    c = {"workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 and 4 deg, "
-                     "plain FP64, batched in one launch",
-         "cells_per_solve": 384 * 96, "solves": len(ALPHAS), "model": "k-omega SST",
+def polar_config(extra=None):
+    c = {"workload": POLAR_NAME, "solves": len(POLAR),
+         "cells": sum(_cells(level) for _, _, _, level, _ in POLAR), "model": "k-omega SST",
          "precision": "fp64 plain (reference-parity form)",
-         "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"}
+         "l2": "state 3.2 GB > L2; a 256 MiB buffer is also written between timed steps",
+         "parallelism": "replicas"}
     if extra:
         c.update(extra)
     return c
+
+
+def _cells(level: str) -> int:
+    s, w, n = GRIDS[level]
+    return (2 * w + 2 * s - 2) * (n - 1)  # cellsI = 2 wake + 2 surface - 2
 
 
 # ---------------------------------------------------------------- clocks ---
@@ -120,51 +145,52 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- workload ---
 
-def build_solvers(cb, precision: int = 0):
-    mesh = cb.cgrid(WORKLOAD["designation"], **{k: v for k, v in WORKLOAD.items() if k != "designation"})
+def _mesh(cb, designation, level, first_layer, cache):
+    key = (designation, level, first_layer)
+    if key not in cache:
+        sp, wp, npn = GRIDS[level]
+        cache[key] = cb.cgrid(designation, surface_points=sp, wake_points=wp, normal_points=npn,
+                              first_layer_height=first_layer, **EXTENTS)
+    return cache[key]
+
+
+def polar_solvers(cb, precision: int = 0, cluster: int | None = None):
+    """The 24 solves of the batched polar, created on the device from the
+    uniform start. `cluster` fixes the CTAs per solve (the library's
+    CFD_CLUSTER_SIZE knob), else each solve takes the library's default."""
     settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
                                     precision=precision)
-    solvers = []
-    for alpha in ALPHAS:
+    previous = os.environ.get("CFD_CLUSTER_SIZE")
+    if cluster is not None:
+        os.environ["CFD_CLUSTER_SIZE"] = str(cluster)
+    meshes, solvers = {}, []
+    try:
+        for des, alpha, re, level, fl in POLAR:
+            mesh = _mesh(cb, des, level, fl, meshes)
+            s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
+            s.set_turbulence_model(cb.MODEL_SST)
+            s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, re))
+            solvers.append(s)
+    finally:
+        if cluster is not None:
+            if previous is None:
+                os.environ.pop("CFD_CLUSTER_SIZE", None)
+            else:
+                os.environ["CFD_CLUSTER_SIZE"] = previous
+    return solvers
+
+
+def c2_solvers(cb, precision: int = 0):
+    """The 384x96 NACA 0012 pair (alpha 0 and 4) of --workload c2."""
+    mesh = _mesh(cb, "0012", "medium", 1e-5, {})
+    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
+                                    precision=precision)
+    out = []
+    for alpha in C2_ALPHAS:
         s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
         s.set_turbulence_model(cb.MODEL_SST)
         s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, REYNOLDS))
-        solvers.append(s)
-    return mesh, solvers
-
-
-def converge_both_forms(cb, tolerance: float = 1e-6, cap: int = 6000) -> dict:
-    """The benchmark pair solved to convergence in each form from the uniform
-    start, batched (both solves in one launch per chunk, each stopping on its
-    own): solves/min, iterations, and the mixed answers' differences from
-    the FP64 ones (Cl, Cd, Cm, and Cp at every station)."""
-    import torch
-    out = {"tolerance": tolerance, "cap": cap}
-    answers = {}
-    for name, precision in (("plain", 0), ("mixed", 1)):
-        mesh, solvers = build_solvers(cb, precision)
-        batch = cb.Batch(solvers)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        taken, _ = batch.iterate(cap, tolerance)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
-        forces = [s.forces(1.0, a, 1.0) for s, a in zip(solvers, ALPHAS)]
-        answers[name] = forces
-        out[name] = {"solves_per_min": 60.0 * len(solvers) / wall, "wall_s": wall,
-                     "iterations": list(taken),
-                     "cl": [f[0].lift_coefficient for f in forces],
-                     "cd": [f[0].drag_coefficient for f in forces]}
-        batch.close()
-        for s in solvers:
-            s.close()
-    p, m = answers["plain"], answers["mixed"]
-    out["mixed_vs_plain"] = {
-        "solves_per_min_ratio": out["mixed"]["solves_per_min"] / out["plain"]["solves_per_min"],
-        "dcl": [abs(b[0].lift_coefficient - a[0].lift_coefficient) for a, b in zip(p, m)],
-        "dcd": [abs(b[0].drag_coefficient - a[0].drag_coefficient) for a, b in zip(p, m)],
-        "dcm": [abs(b[0].moment_coefficient - a[0].moment_coefficient) for a, b in zip(p, m)],
-        "dcp_inf": [float(np.max(np.abs(b[1] - a[1]))) for a, b in zip(p, m)]}
+        out.append(s)
     return out
 
 
@@ -177,9 +203,9 @@ def measured_peak() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
-def committed_traffic(name: str = "simple_kernel_c2_sst_fp64.md") -> float | None:
-    """DRAM bytes per launch of simpleKernel on this workload, from the
-    committed ncu summary (its `traffic_bytes_per_launch:` line)."""
+def committed_traffic(name: str) -> float | None:
+    """DRAM bytes per launch of simpleKernel on a workload, from a committed
+    ncu summary (its `traffic_bytes_per_launch:` line)."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         with open(path) as f:
@@ -191,82 +217,205 @@ def committed_traffic(name: str = "simple_kernel_c2_sst_fp64.md") -> float | Non
     return None
 
 
+def algorithmic_bytes(solvers, cg_iterations, mixed: bool) -> float:
+    """Bytes one batched launch of one iteration must move (bytes_model), summed
+    over the solves with each solve's executed CG (or inner multigrid-CG)
+    iterations."""
+    import bytes_model
+    total = 0.0
+    for s, n in zip(solvers, cg_iterations):
+        per = (bytes_model.bytes_per_cell_iteration_mixed(True, n) if mixed
+               else bytes_model.bytes_per_cell_iteration(True, n))
+        total += per * s.mesh.cells
+    return total
+
+
 # ------------------------------------------------------------- CPU leg ---
 
 def _ref_worker(args):
-    """One process: the reference solver (or the oracle port) on one solve,
-    `warm` untimed then `count` timed iterations. Returns (cells, seconds, kind)."""
-    alpha, warm, count = args
+    """One process: the reference solver (or, where it was not built, the
+    oracle port) on a list of solves: `warm` untimed, then `count` timed
+    iterations of every solve, round-robin like one batched step after
+    another. Returns (cells, seconds, kind)."""
+    solves, warm, count = args
     sys.path.insert(0, ROOT)
     sys.path.insert(0, PKG)
     from oracle import reference as R
-    w = WORKLOAD
     settings = np.array([0.5, 0.2, 3, 200, 0.01, 0, 0.5, INTENSITY, VISCOSITY_RATIO, 0.0, 1, 1.0])
-    if R.available():
-        m = R.RefMesh.cgrid(w["designation"], w["surface_points"], w["wake_points"],
-                            w["normal_points"], w["first_layer_height"], w["upstream_chords"],
-                            w["downstream_chords"], w["vertical_chords"])
-        kind, vel, pres = m.conditions(1.0, alpha, 1.0, REYNOLDS)
-        s = R.RefSolver(m, kind, vel, pres, settings, turbulence=2)
-        s.initialise(*m.uniform(1.0, alpha, 1.0, REYNOLDS))
-        label = "reference"
-    else:
-        import cfd_b200 as cb
-        from oracle import port
-        m = cb.cgrid(w["designation"], **{k: v for k, v in w.items() if k != "designation"})
-        s = port.OracleSolver(m, cb.freestream_conditions(m, 1.0, alpha), settings, 2,
-                              port.LEXICOGRAPHIC)
-        s.initialise(*cb.uniform_field(m, 1.0, alpha, 1.0, REYNOLDS))
-        label = "port"
-    s.iterate(warm)
+    built = []
+    for des, alpha, re, level, fl in solves:
+        sp, wp, npn = GRIDS[level]
+        if R.available():
+            m = R.RefMesh.cgrid(des, sp, wp, npn, fl, EXTENTS["upstream_chords"],
+                                EXTENTS["downstream_chords"], EXTENTS["vertical_chords"])
+            kind, vel, pres = m.conditions(1.0, alpha, 1.0, re)
+            s = R.RefSolver(m, kind, vel, pres, settings, turbulence=2)
+            s.initialise(*m.uniform(1.0, alpha, 1.0, re))
+            label = "reference"
+        else:
+            import cfd_b200 as cb
+            from oracle import port
+            m = cb.cgrid(des, surface_points=sp, wake_points=wp, normal_points=npn,
+                         first_layer_height=fl, **EXTENTS)
+            s = port.OracleSolver(m, cb.freestream_conditions(m, 1.0, alpha), settings, 2,
+                                  port.LEXICOGRAPHIC)
+            s.initialise(*cb.uniform_field(m, 1.0, alpha, 1.0, re))
+            label = "port"
+        built.append((m, s))
+    for _ in range(warm):
+        for _, s in built:
+            s.iterate(1)
     t0 = time.perf_counter()
-    s.iterate(count)
-    return m.cells, time.perf_counter() - t0, label
+    for _ in range(count):
+        for _, s in built:
+            s.iterate(1)
+    return sum(m.cells for m, _ in built), time.perf_counter() - t0, label
 
 
-def cpu_baseline(iterations: int = 60) -> dict:
-    """The reference CPU solver on one core: a bounded sample of the workload
-    (one of its solves, `iterations` outer iterations after 3 warm-up)."""
-    cells, seconds, kind = _ref_worker((ALPHAS[-1], 3, iterations))
-    return {"value": cells * iterations / seconds, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"{iterations} SIMPLE iterations of one 384x96 SST solve (alpha {ALPHAS[-1]}), "
-                      f"single thread, {seconds:.1f} s"}
+def _processes(work: int) -> int:
+    return max(1, min(os.cpu_count() or 1, work))
+
+
+def cpu_baseline(iterations: int = 10) -> dict:
+    """The reference CPU solver on the host's cores: a bounded sample of the
+    workload, one fine-grid solve of the polar per process (768x192 NACA 2412,
+    a different incidence in each), 2 untimed then `iterations` timed outer
+    iterations; the aggregate rate is every process's cells x iterations over
+    the slowest process's time."""
+    import multiprocessing as mp
+    fine = [p for p in POLAR if p[3] == "fine"]
+    procs = _processes(len(fine))
+    jobs = [([fine[k]], 2, iterations) for k in range(procs)]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        results = pool.map(_ref_worker, jobs)
+    cells = sum(r[0] for r in results)
+    slowest = max(r[1] for r in results)
+    return {"value": cells * iterations / slowest, "unit": UNIT, "cores": procs, "kind": results[0][2],
+            "sample": f"{procs} processes, one 768x192 NACA 2412 SST solve each (alpha "
+                      f"{fine[0][1]:g}..{fine[procs - 1][1]:g}), {iterations} timed iterations after 2, "
+                      f"slowest {slowest:.1f} s"}
 
 
 def run_reference_arm(args) -> None:
+    """The reference's CPU solver on the same 24-solve workload: the solves
+    are dealt round-robin to one process per host core (at most one per
+    solve); a step is one outer iteration of every solve."""
     import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    procs = max(1, min(cores, 64))
-    per_step = 1
-    count = max(1, args.steps) * per_step
-    jobs = [(ALPHAS[k % len(ALPHAS)], args.warmup, count) for k in range(procs)]
-    ctx = mp.get_context("spawn")
+    workload = POLAR if args.workload != "c2" else [("0012", a, REYNOLDS, "medium", 1e-5) for a in C2_ALPHAS]
+    procs = _processes(len(workload))
+    count = max(1, args.steps)
+    jobs = [([workload[k] for k in range(p, len(workload), procs)], args.warmup, count)
+            for p in range(procs)]
     t0 = time.perf_counter()
-    with ctx.Pool(procs) as pool:
+    with mp.get_context("spawn").Pool(procs) as pool:
         results = pool.map(_ref_worker, jobs)
     wall = time.perf_counter() - t0
     cells = sum(r[0] for r in results)
     slowest = max(r[1] for r in results)
     value = cells * count / slowest
     kind = results[0][2]
+    config = polar_config({"processes": procs}) if args.workload != "c2" else c2_config({"processes": procs})
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": slowest / count * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": config({"processes": procs}),
+        "data": "synthetic", "config": config,
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
-                         "sample": f"{procs} independent solves (alpha {ALPHAS}) x {count} timed "
-                                   f"iterations after {args.warmup} warm-up, one process per core; "
-                                   f"wall {wall:.1f} s"},
+                         "sample": f"{len(workload)} solves over {procs} processes (one per core), "
+                                   f"{count} timed steps after {args.warmup} warm-up, each step one "
+                                   f"iteration of every solve; wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+def c2_config(extra=None):
+    c = {"workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 and 4 deg, "
+                     "plain FP64, batched in one launch",
+         "cells_per_solve": 384 * 96, "solves": len(C2_ALPHAS), "model": "k-omega SST",
+         "precision": "fp64 plain (reference-parity form)",
+         "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
 # ------------------------------------------------------------- GPU arm ---
+
+def _timed_steps(torch, batch, handle, stream, flush, steps, warmup, dist, launch=None):
+    """W untimed then K timed one-iteration launches of a batch, each bracketed
+    by CUDA events on the launching stream, the L2 flush between them."""
+    launch = launch or batch.launch
+    for _ in range(warmup):
+        flush.zero_()
+        launch(1, handle)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            launch(1, handle)
+            ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    return np.array([a.elapsed_time(b) for a, b in zip(starts, ends)]), clocks.summary()
+
+
+def _e2e(torch, batch, solvers, steps, dist):
+    """The metric through the C ABI with host buffers: every step loads each
+    solve's state from pinned host memory, iterates the batch once, and reads
+    each solve's u, v and p back into pinned host memory. Returns (seconds,
+    h2d bytes per step, d2h bytes per step)."""
+    def pinned(n):
+        return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+    states, outs = [], []
+    for s in solvers:
+        a = {}
+        for name in ("U", "V", "P", "K", "OMEGA", "MUT", "MU_EFF", "MASS_FLUX"):
+            buf = pinned(s.mesh.faces if name == "MASS_FLUX" else s.mesh.cells)
+            s.read_into(name, buf)
+            a[name] = buf
+        states.append(a)
+        outs.append({name: pinned(s.mesh.cells) for name in ("U", "V", "P")})
+    h2d = sum(sum(b.nbytes for b in a.values()) for a in states)
+    d2h = sum(sum(b.nbytes for b in o.values()) for o in outs) + len(solvers) * 136
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for s, a in zip(solvers, states):
+            s.load_state(u=a["U"], v=a["V"], p=a["P"], mass_flux=a["MASS_FLUX"], k=a["K"],
+                         omega=a["OMEGA"], mut=a["MUT"], mu_eff=a["MU_EFF"])
+        taken, _ = batch.iterate(1)
+        assert all(t == 1 for t in taken)
+        for s, o in zip(solvers, outs):
+            for name, buf in o.items():
+                s.read_into(name, buf)
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0, h2d, d2h
+
+
+def _roofline(solvers, cg, step_ms, mixed, profile):
+    peak, peak_kind = measured_peak()
+    per_launch = algorithmic_bytes(solvers, cg, mixed)
+    achieved = per_launch / (float(np.mean(step_ms)) / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "traffic": committed_traffic(profile), "kernel": "simpleKernel",
+            "bytes_per_launch_algorithmic": per_launch,
+            "mean_cg_iterations": float(np.average(cg, weights=[s.mesh.cells for s in solvers]))}
+
 
 def run_ours(args) -> None:
     import torch
@@ -280,17 +429,21 @@ def run_ours(args) -> None:
 
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     else:
         torch.cuda.set_device(0)
 
     import cfd_b200 as cb
     cb.set_device(torch.cuda.current_device())
-    mixed = args.form == "mixed"
-    mesh, solvers = build_solvers(cb, 1 if mixed else 0)
+    c2 = args.workload == "c2"
+    mixed_only = args.form == "mixed"
+    if c2:
+        solvers = c2_solvers(cb, 1 if mixed_only else 0)
+    else:
+        solvers = polar_solvers(cb, 1 if mixed_only else 0, MIXED_CLUSTER if mixed_only else None)
     batch = cb.Batch(solvers)
-    cells = mesh.cells * len(solvers)
+    cells = sum(s.mesh.cells for s in solvers)
     # A stream of our own: events, the L2 flush and the solver launches all go
     # on it (torch's default stream is the legacy NULL stream, handle 0).
     stream = torch.cuda.Stream()
@@ -299,118 +452,82 @@ def run_ours(args) -> None:
     assert handle != 0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    # warm-up (untimed), also moves the flow off its uniform start
     launch = batch.graph_launch if args.graph else batch.launch
-    for _ in range(args.warmup):
-        flush.zero_()
-        launch(1, handle)
-    torch.cuda.synchronize()
-
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(torch.cuda.current_device()) as clocks:
-        for k in range(args.steps):
-            flush.zero_()
-            starts[k].record(stream)
-            launch(1, handle)
-            ends[k].record(stream)
-        torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    step_ms = np.array([s.elapsed_time(e) for s, e in zip(starts, ends)])
+    step_ms, clocks = _timed_steps(torch, batch, handle, stream, flush, args.steps, args.warmup, dist,
+                                   launch)
     total_s = float(step_ms.sum()) / 1e3
-    gpu_launches = args.steps
     _, monitors = batch.monitors()
     finite = all(math.isfinite(m.continuity) for m in monitors)
+    cg = [float(m.pressure_iterations) for m in monitors]  # executed in the last timed step
+    shape = list(batch.shape())
 
-    # mean executed CG iterations: 20 more iterations with history
-    cg = []
-    for s in solvers:
-        _, hist = s.iterate(20, history=True)
-        cg.extend(hist[:, 5].tolist())
-    mean_cg = float(np.mean(cg))
+    e2e_steps = max(3, min(10, args.steps))
+    e2e_s, h2d, d2h = _e2e(torch, batch, solvers, e2e_steps, dist)
 
-    # e2e through the C ABI from pinned host buffers
-    e2e_steps = max(5, min(50, args.steps))
-    states = []
-    for s in solvers:
-        arrays = {}
-        for name in ("U", "V", "P", "K", "OMEGA", "MUT", "MU_EFF"):
-            t = torch.empty(mesh.cells, dtype=torch.float64, pin_memory=True)
-            t.numpy()[:] = s.read(name)
-            arrays[name] = t
-        t = torch.empty(mesh.faces, dtype=torch.float64, pin_memory=True)
-        t.numpy()[:] = s.read("MASS_FLUX")
-        arrays["MASS_FLUX"] = t
-        states.append(arrays)
-    h2d = sum(sum(t.numel() * 8 for t in a.values()) for a in states)
-    d2h = len(solvers) * 136
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        for s, a in zip(solvers, states):
-            s.load_state(u=a["U"].numpy(), v=a["V"].numpy(), p=a["P"].numpy(),
-                         mass_flux=a["MASS_FLUX"].numpy(), k=a["K"].numpy(),
-                         omega=a["OMEGA"].numpy(), mut=a["MUT"].numpy(), mu_eff=a["MU_EFF"].numpy())
-        taken, mons = batch.iterate(1)
-        assert all(t == 1 for t in taken)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-
+    # the mixed FP32/FP64 form on the same workload (its own batch)
+    mixed = None
+    if not mixed_only and not c2 and not args.no_mixed:
+        batch.close()
+        for s in solvers:
+            s.close()
+        m_solvers = polar_solvers(cb, 1, MIXED_CLUSTER)
+        m_batch = cb.Batch(m_solvers)
+        m_ms, m_clocks = _timed_steps(torch, m_batch, handle, stream, flush, args.steps, args.warmup, dist)
+        _, m_mon = m_batch.monitors()
+        m_inner = [float(m.pressure_iterations) for m in m_mon]
+        m_total = float(m_ms.sum()) / 1e3
+        mixed = {"ms_per_step": float(np.mean(m_ms)), "total_s": m_total, "shape": list(m_batch.shape()),
+                 "clocks": m_clocks, "inner": m_inner, "solvers": m_solvers,
+                 "finite": all(math.isfinite(m.continuity) for m in m_mon)}
+        m_batch.close()
     # multi-rank: max time over ranks, cells summed
+    times = [total_s, e2e_s] + ([mixed["total_s"]] if mixed else [])
     if dist is not None:
-        (total_s, e2e_s), all_cells = reduce_over_ranks([total_s, e2e_s], cells, dist, "cuda")
+        times, all_cells = reduce_over_ranks(times, cells, dist, "cuda")
     else:
         all_cells = float(cells)
-    value = all_cells * args.steps / total_s
-    e2e_value = all_cells * e2e_steps / e2e_s
+    value = all_cells * args.steps / times[0]
+    e2e_value = all_cells * e2e_steps / times[1]
 
     if rank == 0:
-        import bytes_model
-        peak, peak_kind = measured_peak()
-        if mixed:
-            per_launch_bytes = bytes_model.bytes_per_cell_iteration_mixed(True, mean_cg) * cells
-        else:
-            per_launch_bytes = bytes_model.bytes_per_cell_iteration(True, mean_cg) * cells
-        mean_launch_s = float(np.mean(step_ms)) / 1e3
-        achieved = per_launch_bytes / mean_launch_s / 1e9
-        traffic = committed_traffic("simple_kernel_c2_sst_mixed.md" if mixed else "simple_kernel_c2_sst_fp64.md")
-        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                    "traffic": traffic,
-                    "kernel": "simpleKernel", "bytes_per_launch_algorithmic": per_launch_bytes,
-                    "mean_cg_iterations": mean_cg}
+        profile = ("simple_kernel_c2_sst_mixed.md" if mixed_only else "simple_kernel_c2_sst_fp64.md") if c2 \
+            else ("simple_kernel_polar_mixed.md" if mixed_only else "simple_kernel_polar_fp64.md")
+        roofline = _roofline(solvers, cg, step_ms, mixed_only, profile)
+        config = c2_config() if c2 else polar_config()
+        config.update({"cluster_shape": shape, "launch": "cuda graph" if args.graph else "direct",
+                       "cg_iterations_per_solve": cg})
+        if mixed_only:
+            config["precision"] = "mixed: FP64 assembly/state, FP32 sweeps and multigrid CG"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": float(np.mean(step_ms)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32/f64" if mixed else "f64",
-            "data": "synthetic",
-            "config": config({"cluster_shape": list(batch.shape()), "launch": "cuda graph" if args.graph else "direct"}
-                             if not mixed else
-                             {"cluster_shape": list(batch.shape()),
-                              "workload": "NACA0012 k-omega SST Re1e6 C-grid 384x96 (medium), alpha 0 "
-                                          "and 4 deg, mixed FP32/FP64 form, batched in one launch",
-                              "precision": "mixed: FP64 assembly/state, FP32 sweeps and multigrid CG"}),
+            "dtype": "f32/f64" if mixed_only else "f64", "data": "synthetic", "config": config,
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": gpu_launches, "clocks": clocks.summary(),
-            "finite": finite,
+            "gpu_launches": args.steps, "clocks": clocks, "finite": finite,
         }
+        if mixed is not None:
+            m_value = all_cells * args.steps / times[2]
+            line["mixed"] = {
+                "value": m_value, "unit": UNIT, "ms_per_step": mixed["ms_per_step"],
+                "vs_plain": m_value / value, "cluster_shape": mixed["shape"], "dtype": "f32/f64",
+                "inner_iterations_per_solve": mixed["inner"], "clocks": mixed["clocks"],
+                "finite": mixed["finite"],
+                "roofline": _roofline(mixed["solvers"], mixed["inner"], np.array([mixed["ms_per_step"]]),
+                                      True, "simple_kernel_polar_mixed.md")}
+            for s in mixed["solvers"]:
+                s.close()
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
-        if world == 1 and not args.no_convergence:
-            line["convergence"] = converge_both_forms(cb)
+        if world == 1 and not args.no_convergence and not c2:
+            line["polar"] = polar_to_tolerance(cb, args.tolerance, args.cap, args.chunk)
         print(json.dumps(line), flush=True)
-    batch.close()
-    for s in solvers:
-        s.close()
+    if mixed is None:
+        batch.close()
+        for s in solvers:
+            s.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -428,11 +545,6 @@ def reduce_over_ranks(times, cells, dist, device):
 
 
 # ------------------------------------------------- engine workloads ---
-
-GRIDS = {  # (surface, wake, normal) points; cells 192x48, 384x96, 768x192
-    "coarse": (64, 33, 49), "medium": (128, 65, 97), "fine": (256, 129, 193),
-}
-
 
 def _percentiles(values):
     if not values:
@@ -453,40 +565,29 @@ def _summarise(results, wall_s, cb):
             "iterations": _percentiles([r.iterations for r in results])}
 
 
-def _polar_requests(cb, args, precision):
-    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO, precision=precision)
+def _polar_requests(cb, tolerance, cap, precision):
+    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
+                                    precision=precision)
     reqs = []
-    for alpha in range(-4, 17):
-        s, w, n = GRIDS["fine"]
-        reqs.append(cb.request("2412", float(alpha), 3e6, tolerance=args.tolerance,
-                               max_iterations=args.cap, surface_points=s, wake_points=w,
-                               normal_points=n, first_layer_height=5e-6, settings=settings))
-    for level, fl in (("coarse", 2e-3), ("medium", 1e-5), ("fine", 5e-6)):
-        s, w, n = GRIDS[level]
-        reqs.append(cb.request("0012", 4.0, 1e6, tolerance=args.tolerance, max_iterations=args.cap,
-                               surface_points=s, wake_points=w, normal_points=n,
+    for des, alpha, re, level, fl in POLAR:
+        sp, wp, npn = GRIDS[level]
+        reqs.append(cb.request(des, alpha, re, tolerance=tolerance, max_iterations=cap,
+                               surface_points=sp, wake_points=wp, normal_points=npn,
                                first_layer_height=fl, settings=settings))
     return reqs
 
 
-def run_polar(args) -> None:
-    """21-point NACA 2412 SST Re 3e6 polar (alpha -4..16 step 1) on
-    the fine 768x192 C-grid, plus NACA 0012 SST Re 1e6 alpha 4 on the coarse,
-    medium and fine grids, all resident at once in one engine; run in the
-    plain FP64 form and in the mixed FP32/FP64 form, with the mixed answers'
-    differences from the FP64 ones (Cl, Cd, Cm, and Cp at every station)."""
-    import torch
-    torch.cuda.set_device(0)
-    import cfd_b200 as cb
-    cb.set_device(0)
-    forms = ("plain", "mixed") if args.precision == "both" else (args.precision,)
-    out = {"workload": "polar: NACA2412 SST Re3e6 768x192 alpha -4..16 + NACA0012 SST Re1e6 "
-                       "alpha 4 on 192x48/384x96/768x192", "tolerance": args.tolerance,
-           "cap": args.cap, "chunk": args.chunk}
+def polar_to_tolerance(cb, tolerance, cap, chunk, forms=("plain", "mixed"), csv_prefix=""):
+    """The 24 solves of the batched polar, each solved to worst residual <
+    `tolerance` (or `cap` iterations) in the solve engine, in each form:
+    solves/min, time-to-convergence percentiles, and per solve the mixed
+    form's Cl/Cd/Cm and L-inf Cp differences from the plain FP64 form (which
+    the parity tests tie to the FP64 oracle)."""
+    out = {"workload": POLAR_NAME, "tolerance": tolerance, "cap": cap, "chunk": chunk}
     runs = {}
     for form in forms:
-        reqs = _polar_requests(cb, args, 0 if form == "plain" else 1)
-        engine = cb.Engine(chunk=args.chunk)
+        reqs = _polar_requests(cb, tolerance, cap, 0 if form == "plain" else 1)
+        engine = cb.Engine(chunk=chunk)
         t0 = time.perf_counter()
         results = sorted(engine.run(reqs), key=lambda r: r.id)
         wall = time.perf_counter() - t0
@@ -494,17 +595,16 @@ def run_polar(args) -> None:
         engine.close()
         runs[form] = (results, cps)
         summary = _summarise(results, wall, cb)
-        if args.csv:
+        if csv_prefix:
             sweep = [r for r in results if reqs[r.id].designation.decode() == "2412"]
-            with open(f"{args.csv}_{form}.csv", "w") as fh:
+            with open(f"{csv_prefix}_{form}.csv", "w") as fh:
                 fh.write(cb.polar_csv(sweep, [reqs[r.id].alpha_deg for r in sweep], "NACA 2412",
                                       "768x192", 3e6, 1.0))
-        summary["polar"] = [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
-                             "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
-                             "iterations": r.iterations, "ctas": r.cluster_size,
-                             "cl": r.lift_coefficient,
-                             "cd": r.drag_coefficient, "cm": r.moment_coefficient,
-                             "continuity": r.continuity} for r in results]
+        summary["points"] = [{"alpha": reqs[r.id].alpha_deg, "section": reqs[r.id].designation.decode(),
+                              "cells": r.cells, "status": cb.STATUS_NAMES[r.status],
+                              "iterations": r.iterations, "ctas": r.cluster_size,
+                              "cl": r.lift_coefficient, "cd": r.drag_coefficient,
+                              "cm": r.moment_coefficient} for r in results]
         out[form] = summary
     if len(forms) == 2:
         (rp, cpp), (rm, cpm) = runs["plain"], runs["mixed"]
@@ -513,19 +613,33 @@ def run_polar(args) -> None:
             row = {"id": a.id, "dcl": abs(b.lift_coefficient - a.lift_coefficient),
                    "dcd": abs(b.drag_coefficient - a.drag_coefficient),
                    "dcm": abs(b.moment_coefficient - a.moment_coefficient),
+                   "status_plain": cb.STATUS_NAMES[a.status], "status_mixed": cb.STATUS_NAMES[b.status],
                    "iterations_plain": a.iterations, "iterations_mixed": b.iterations}
             if a.id in cpp and b.id in cpm and len(cpp[a.id]) == len(cpm[b.id]):
                 row["dcp_inf"] = float(np.max(np.abs(cpm[b.id] - cpp[a.id])))
             rows.append(row)
-        both_converged = [r for r, a, b in zip(rows, rp, rm) if a.status == 0 and b.status == 0]
+        both = [r for r, a, b in zip(rows, rp, rm) if a.status == 0 and b.status == 0]
         out["mixed_vs_plain"] = {
             "solves_per_min_ratio": out["mixed"]["solves_per_min"] / out["plain"]["solves_per_min"],
             "max_dcl": max(r["dcl"] for r in rows), "max_dcd": max(r["dcd"] for r in rows),
             "max_dcm": max(r["dcm"] for r in rows),
             "max_dcp_inf": max((r.get("dcp_inf", 0.0) for r in rows), default=None),
-            "max_dcl_both_converged": max((r["dcl"] for r in both_converged), default=None),
+            "both_converged": len(both),
+            "max_dcl_both_converged": max((r["dcl"] for r in both), default=None),
+            "max_dcd_both_converged": max((r["dcd"] for r in both), default=None),
             "per_solve": rows}
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_polar(args) -> None:
+    """The batched polar solved to convergence, alone (its JSON line only)."""
+    import torch
+    torch.cuda.set_device(0)
+    import cfd_b200 as cb
+    cb.set_device(0)
+    forms = ("plain", "mixed") if args.precision == "both" else (args.precision,)
+    print(json.dumps(polar_to_tolerance(cb, args.tolerance, args.cap, args.chunk, forms, args.csv)),
+          flush=True)
 
 
 def run_settled(args) -> None:
@@ -631,14 +745,17 @@ def run_serve(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-convergence", action="store_true",
-                    help="skip solving the pair to convergence in both forms")
-    ap.add_argument("--workload", choices=("c2", "polar", "serve", "settled"), default="c2",
-                    help="c2: the benchmark line (default); polar / serve / settled: engine workloads")
+                    help="skip solving the polar to convergence in both forms")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip timing the mixed form's batch")
+    ap.add_argument("--workload", choices=("batch", "c2", "polar", "serve", "settled"), default="batch",
+                    help="batch: the benchmark line, the 24-solve polar in one launch per step "
+                         "(default); c2: the 384x96 pair; polar / serve / settled: engine workloads")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--cap", type=int, default=4000)
     ap.add_argument("--chunk", type=int, default=32)
@@ -649,9 +766,9 @@ def main() -> None:
                     help="polar: write the 2412 sweep of each form as <prefix>_<form>.csv "
                          "in the reference's polar CSV layout")
     ap.add_argument("--graph", action="store_true",
-                    help="c2: replay each step's launch from a CUDA graph")
+                    help="batch / c2: replay each step's launch from a CUDA graph")
     ap.add_argument("--form", choices=("plain", "mixed"), default="plain",
-                    help="c2: the form the benchmark line times (plain FP64 by default)")
+                    help="batch / c2: the form the benchmark line times (plain FP64 by default)")
     ap.add_argument("--precision", choices=("plain", "mixed", "both"), default="both",
                     help="polar: which form(s) to run; serve: plain unless 'mixed'")
     args = ap.parse_args()

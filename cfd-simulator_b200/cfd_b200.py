@@ -191,6 +191,8 @@ _sig("cfd_cg_solve", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
 _sig("cfd_cg_solve_noalloc", C.c_int, _P, _P, C.c_double, C.c_int, _P, _P)
 _sig("cfd_engine_create", C.c_int, C.c_ulonglong, C.c_int, _P)
 _sig("cfd_engine_submit", C.c_int, _P, _P, _P)
+_sig("cfd_engine_submit_sweep", C.c_int, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int, _P, _P)
+_sig("cfd_sweep_angles", C.c_int, C.c_double, C.c_double, C.c_double, _P, C.c_int, _P)
 _sig("cfd_engine_step", C.c_int, _P, _P, _P)
 _sig("cfd_engine_results", C.c_int, _P, _P, C.c_int, _P)
 _sig("cfd_engine_surface", C.c_int, _P, C.c_int, _P, C.c_int, _P)
@@ -413,12 +415,20 @@ class SimpleSolver:
         _check(_lib.cfd_gpu_iterate_partial(self._h, code, C.byref(last)))
         return last
 
-    def read(self, name: str) -> np.ndarray:
+    def _size(self, name: str) -> int:
         n = self.mesh.cells
-        size = self.mesh.faces if name in FACE_FIELDS else (2 * n if name in VEC2_FIELDS else n)
-        out = np.zeros(size)
+        return self.mesh.faces if name in FACE_FIELDS else (2 * n if name in VEC2_FIELDS else n)
+
+    def read(self, name: str) -> np.ndarray:
+        out = np.zeros(self._size(name))
         _check(_lib.cfd_gpu_read_field(self._h, FIELD[name], _ptr(out)))
         return out
+
+    def read_into(self, name: str, out: np.ndarray) -> None:
+        """read() into a caller's float64 buffer (e.g. pinned host memory)."""
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self._size(name):
+            raise ValueError(f"{name} needs a contiguous float64 buffer of {self._size(name)} values")
+        _check(_lib.cfd_gpu_read_field(self._h, FIELD[name], _ptr(out)))
 
     def load_state(self, u=None, v=None, p=None, mass_flux=None, k=None, omega=None, mut=None,
                    mu_eff=None) -> None:
@@ -557,13 +567,23 @@ class Result(C.Structure):
                 ("friction_drag_coefficient", C.c_double), ("submitted_s", C.c_double),
                 ("started_s", C.c_double), ("finished_s", C.c_double),
                 ("separation_upper_chord_fraction", C.c_double),
-                ("separation_lower_chord_fraction", C.c_double)]
+                ("separation_lower_chord_fraction", C.c_double), ("alpha_deg", C.c_double),
+                ("continued", C.c_int), ("error", C.c_int)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
-STATUS_NAMES = {0: "converged", 1: "iteration-limit", 2: "diverged"}
+STATUS_NAMES = {0: "converged", 1: "iteration-limit", 2: "diverged", 3: "failed"}
+
+
+def sweep_angles(start: float, end: float, step: float) -> list[float]:
+    """post::sweepAngles (Polar.cpp:36-77) through the C ABI."""
+    n = C.c_int()
+    _check(_lib.cfd_sweep_angles(start, end, step, None, 0, C.byref(n)))
+    out = np.zeros(max(n.value, 1))
+    _check(_lib.cfd_sweep_angles(start, end, step, _ptr(out), n.value, C.byref(n)))
+    return out[: n.value].tolist()
 
 
 def request(designation: str, alpha_deg: float, reynolds: float, model: int = MODEL_SST,
@@ -609,6 +629,15 @@ class Engine:
         _check(_lib.cfd_engine_submit(self._h, C.byref(req), C.byref(out)))
         return out.value
 
+    def submit_sweep(self, base: Request, start: float, end: float, step: float,
+                     continued: bool = True) -> list[int]:
+        """A polar sweep run point after point (cfd_engine_submit_sweep): the
+        ids of its points, in sweep order."""
+        first, count = C.c_int(), C.c_int()
+        _check(_lib.cfd_engine_submit_sweep(self._h, C.byref(base), start, end, step,
+                                            1 if continued else 0, C.byref(first), C.byref(count)))
+        return list(range(first.value, first.value + count.value))
+
     def step(self) -> tuple[int, int]:
         a, q = C.c_int(), C.c_int()
         _check(_lib.cfd_engine_step(self._h, C.byref(a), C.byref(q)))
@@ -635,6 +664,10 @@ class Engine:
         """Submit everything, step until the engine is empty."""
         for r in requests:
             self.submit(r)
+        return self.drain()
+
+    def drain(self) -> list[Result]:
+        """Step until every submitted request and sweep has finished."""
         out = []
         while True:
             active, queued = self.step()
@@ -651,15 +684,18 @@ def library_symbols() -> list[str]:
 
 
 # ---- polar CSV ------------------------------------------------------------------------
-def polar_csv(results, alphas, section: str, mesh: str, reynolds: float, speed: float,
-              chord: float = 1.0, moment_reference: float = 0.25,
+def polar_csv(results, alphas=None, section: str = "", mesh: str = "", reynolds: float = 0.0,
+              speed: float = 0.0, chord: float = 1.0, moment_reference: float = 0.25,
               continued_between_points: bool = False) -> str:
     """A polar in the reference's CSV layout (post::toCsv, Polar.cpp:126-164),
     so engine results can be diffed against the reference's examples/*.csv:
     a commented header, then one row per solve in the order given. `results`
-    are engine Results, `alphas` their angles of attack in degrees. Separation
-    is an empty field where the surface stayed attached; l_over_d is 0 where
-    Cd is not positive (AerodynamicForces::liftToDrag, Forces.cpp:50-56)."""
+    are engine Results; `alphas` their angles of attack in degrees (None: each
+    result's own alpha_deg). Separation is an empty field where the surface
+    stayed attached; l_over_d is 0 where Cd is not positive or not finite
+    (AerodynamicForces::liftToDrag, Forces.cpp:50-56)."""
+    if alphas is None:
+        alphas = [r.alpha_deg for r in results]
     lines = ["# cfd_simulator aerodynamic polar",
              f"# section,{section or 'unknown'}",
              f"# mesh,{mesh or 'unknown'}",
@@ -679,8 +715,10 @@ def polar_csv(results, alphas, section: str, mesh: str, reynolds: float, speed: 
                  if r.separation_upper_chord_fraction >= 0.0 else "")
         lower = (f"{r.separation_lower_chord_fraction:.6f}"
                  if r.separation_lower_chord_fraction >= 0.0 else "")
+        # pointStatus: a point that never started has no converged flag set
+        status = "diverged" if r.status == 2 else ("converged" if r.status == 0 else "iteration-limit")
         lines.append(f"{alpha:.6f},{r.lift_coefficient:.8f},{cd:.8f},"
                      f"{r.pressure_drag_coefficient:.8f},{r.friction_drag_coefficient:.8f},"
                      f"{r.moment_coefficient:.8f},{l_over_d:.6f},{upper},{lower},"
-                     f"{STATUS_NAMES[r.status]},{r.iterations},{r.continuity:.6e}")
+                     f"{status},{r.iterations},{r.continuity:.6e}")
     return "\n".join(lines) + "\n"

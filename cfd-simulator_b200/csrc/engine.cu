@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -42,13 +43,24 @@ Status makeCGrid(const char* designation, const cfd_cgrid_options& o, HostMesh* 
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;  // the double std::numbers::pi rounds to
+constexpr int kMaxSweepPoints = 400;               // post::kMaxSweepPoints (Polar.hpp)
+
+/// A start other than the freestream: the u, v and p a continued polar point
+/// takes over from the previous point (src/app/Panels.cpp:1145-1156).
+struct WarmStart {
+  std::vector<double> u, v, p;
+};
 
 struct Slot {
   int id{0};
   cfd_request request{};
   std::unique_ptr<Solver> solver;
+  std::shared_ptr<const HostMesh> mesh;
   int iterations{0};
   bool retried{false};
+  bool continued{false};
+  int sweep{-1};  // index of the sweep this point belongs to, or -1
+  int point{0};   // its position in that sweep
   double submitted{0.0}, started{0.0};
   std::size_t bytes{0};
 };
@@ -58,6 +70,20 @@ struct Pending {
   cfd_request request{};
   std::shared_ptr<const HostMesh> mesh;
   double submitted{0.0};
+  int sweep{-1};
+  int point{0};
+  std::shared_ptr<const WarmStart> warm;  // null: start from the freestream
+};
+
+/// A polar sweep run point after point (the reference's sweep: startPolarSweep,
+/// updatePolar, src/app/Panels.cpp:1601-1797): one request per angle of
+/// sweepAngles, each started when the one before has retired, from its u and
+/// p when the sweep is continued.
+struct Sweep {
+  cfd_request base{};
+  std::vector<double> angles;
+  int firstId{0};
+  bool continued{false};
 };
 
 using MeshKey = std::tuple<std::string, int, int, int, double, double, double, double>;
@@ -84,6 +110,7 @@ struct Engine {
   int chunk{32};
   int nextId{0};
   std::deque<Pending> queue;
+  std::vector<Sweep> sweeps;
   std::vector<std::unique_ptr<Slot>> active;
   std::vector<cfd_result> done;
   std::map<int, std::vector<double>> surfaces;  // Cp per wall station of each finished solve
@@ -145,7 +172,7 @@ struct Engine {
 
   Status start(const Pending& q, std::unique_ptr<Slot>* out) {
     std::unique_ptr<Solver> solver;
-    if (Status st = makeSolver(q, &solver); st != CFD_OK) return st;
+    if (Status st = makeSolver(q, &solver, q.warm.get()); st != CFD_OK) return st;
     std::pair<int, int> shape;
     if (Status st = tunedShape(q, *solver, &shape); st != CFD_OK) return st;
     if (Status st = solver->setLaunchShape(shape.first, shape.second); st != CFD_OK) return st;
@@ -154,6 +181,10 @@ struct Engine {
     slot->request = q.request;
     slot->bytes = solver->deviceBytes();
     slot->solver = std::move(solver);
+    slot->mesh = q.mesh;
+    slot->continued = (q.warm != nullptr);
+    slot->sweep = q.sweep;
+    slot->point = q.point;
     slot->submitted = q.submitted;
     slot->started = now();
     *out = std::move(slot);
@@ -249,7 +280,7 @@ struct Engine {
     return ok();
   }
 
-  Status makeSolver(const Pending& q, std::unique_ptr<Solver>* out) {
+  Status makeSolver(const Pending& q, std::unique_ptr<Solver>* out, const WarmStart* warm = nullptr) {
     const HostMesh& m = *q.mesh;
     cfd_mesh_desc d;
     describe(m, &d);
@@ -274,13 +305,77 @@ struct Engine {
     if (Status st = Solver::create(d, bc, fromC(q.request.settings), &raw); st != CFD_OK) return st;
     std::unique_ptr<Solver> solver(raw);
     if (Status st = solver->setTurbulence(q.request.model); st != CFD_OK) return st;
+    // FlowField::uniform sets density and viscosity from the freestream; a
+    // continued point then takes only velocity and pressure over
+    // (Panels.cpp:1145-1156).
     std::vector<double> u, v, p, rho, mu;
     uniform(q.request, m.cells, &u, &v, &p, &rho, &mu);
+    if (warm != nullptr && warm->u.size() == u.size()) {
+      u = warm->u;
+      v = warm->v;
+      p = warm->p;
+    }
     if (Status st = solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()); st != CFD_OK) {
       return st;
     }
     *out = std::move(solver);
     return ok();
+  }
+
+  /// The next point of a sweep once point `s` has retired with `status`:
+  /// continued from s's u and p unless the sweep starts each point cold or
+  /// s diverged even after its cold retry (Panels.cpp:1785-1796).
+  void advanceSweep(const Slot& s, int status) {
+    const Sweep& sw = sweeps[static_cast<std::size_t>(s.sweep)];
+    const int next = s.point + 1;
+    if (next >= static_cast<int>(sw.angles.size())) return;
+    Pending q;
+    q.id = sw.firstId + next;
+    q.request = sw.base;
+    q.request.alpha_deg = sw.angles[static_cast<std::size_t>(next)];
+    q.mesh = s.mesh;
+    q.submitted = now();
+    q.sweep = s.sweep;
+    q.point = next;
+    const bool cold = !sw.continued || (s.retried && status == CFD_SOLVE_DIVERGED);
+    if (!cold) {
+      auto warm = std::make_shared<WarmStart>();
+      const std::size_t n = static_cast<std::size_t>(s.solver->cells());
+      warm->u.resize(n);
+      warm->v.resize(n);
+      warm->p.resize(n);
+      if (s.solver->readField(CFD_FIELD_U, warm->u.data()) == CFD_OK &&
+          s.solver->readField(CFD_FIELD_V, warm->v.data()) == CFD_OK &&
+          s.solver->readField(CFD_FIELD_P, warm->p.data()) == CFD_OK) {
+        q.warm = std::move(warm);
+      }
+    }
+    queue.push_front(std::move(q));  // a sweep's next point goes ahead of new requests
+  }
+
+  /// A request that could not start (its solver failed to build or
+  /// initialise): reported with CFD_SOLVE_FAILED and the library's status
+  /// code, never as a physics outcome. A sweep stops there, as the
+  /// reference's does (AbortFailed, Polar.cpp:95-98): its remaining points
+  /// are reported failed too, so every id it was given gets a result.
+  void failStart(const Pending& q, Status code) {
+    cfd_result r{};
+    r.id = q.id;
+    r.status = CFD_SOLVE_FAILED;
+    r.error = code;
+    r.alpha_deg = q.request.alpha_deg;
+    r.separation_upper_chord_fraction = r.separation_lower_chord_fraction = -1.0;
+    r.submitted_s = q.submitted;
+    r.started_s = r.finished_s = now();
+    done.push_back(r);
+    if (q.sweep < 0) return;
+    const Sweep& sw = sweeps[static_cast<std::size_t>(q.sweep)];
+    for (int k = q.point + 1; k < static_cast<int>(sw.angles.size()); ++k) {
+      cfd_result rest = r;
+      rest.id = sw.firstId + k;
+      rest.alpha_deg = sw.angles[static_cast<std::size_t>(k)];
+      done.push_back(rest);
+    }
   }
 
   Status admit() {
@@ -291,13 +386,7 @@ struct Engine {
       if (!active.empty() && used + need > budget) break;
       std::unique_ptr<Slot> slot;
       if (Status st = start(q, &slot); st != CFD_OK) {
-        // a request that cannot start is reported, not retried
-        cfd_result r{};
-        r.id = q.id;
-        r.status = CFD_SOLVE_DIVERGED;
-        r.submitted_s = q.submitted;
-        r.started_s = r.finished_s = now();
-        done.push_back(r);
+        failStart(q, st);
         queue.pop_front();
         continue;
       }
@@ -314,6 +403,8 @@ struct Engine {
     r.status = status;
     r.iterations = s.iterations;
     r.retried_cold = s.retried ? 1 : 0;
+    r.continued = s.continued ? 1 : 0;
+    r.alpha_deg = s.request.alpha_deg;
     r.cells = s.solver->cells();
     r.cluster_size = s.solver->clusterSize();
     r.continuity = mon[kMonContinuity];
@@ -430,6 +521,7 @@ struct Engine {
         }
         if (outcome >= 0) {
           finish(s, outcome, mon);
+          if (s.sweep >= 0) advanceSweep(s, outcome);
           used -= s.bytes;
         } else {
           keep.push_back(std::move(active[k]));
@@ -468,35 +560,49 @@ cfd_status cfd_engine_create(unsigned long long budget, int chunk, cfd_engine* o
   return CFD_OK;
 }
 
-cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* r, int* id) {
-  if (e == nullptr || r == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+namespace {
+
+cfd_status checkRequest(const cfd_request* r) {
   if (!(r->reynolds > 0.0) || !(r->speed > 0.0) || !(r->density > 0.0) || !(r->tolerance >= 0.0) ||
       r->max_iterations < 1 || (r->model != 0 && r->model != 1 && r->model != 2)) {
     return cfdb::fail(CFD_INVALID_ARGUMENT, "invalid request");
   }
-  cfdb::Engine& g = e->engine;
-  const cfdb::MeshKey key = cfdb::keyOf(*r);
-  auto it = g.meshes.find(key);
-  std::shared_ptr<const cfdb::HostMesh> mesh;
-  if (it != g.meshes.end()) {
-    mesh = it->second;
-  } else {
-    auto m = std::make_shared<cfdb::HostMesh>();
-    cfd_cgrid_options o;
-    cfd_default_cgrid_options(&o);
-    o.surface_points = r->grid_surface_points;
-    o.wake_points = r->grid_wake_points;
-    o.normal_points = r->grid_normal_points;
-    o.first_layer_height = r->grid_first_layer_height;
-    o.upstream_chords = r->grid_upstream_chords;
-    o.downstream_chords = r->grid_downstream_chords;
-    o.vertical_chords = r->grid_vertical_chords;
-    char name[9] = {0};
-    std::memcpy(name, r->designation, 8);
-    if (cfd_status st = cfdb::makeCGrid(name, o, m.get()); st != CFD_OK) return st;
-    mesh = m;
-    g.meshes[key] = mesh;
+  return CFD_OK;
+}
+
+/// The request's C-grid, generated on first use and cached per grid.
+cfd_status meshFor(cfdb::Engine& g, const cfd_request& r, std::shared_ptr<const cfdb::HostMesh>* out) {
+  const cfdb::MeshKey key = cfdb::keyOf(r);
+  if (auto it = g.meshes.find(key); it != g.meshes.end()) {
+    *out = it->second;
+    return CFD_OK;
   }
+  auto m = std::make_shared<cfdb::HostMesh>();
+  cfd_cgrid_options o;
+  cfd_default_cgrid_options(&o);
+  o.surface_points = r.grid_surface_points;
+  o.wake_points = r.grid_wake_points;
+  o.normal_points = r.grid_normal_points;
+  o.first_layer_height = r.grid_first_layer_height;
+  o.upstream_chords = r.grid_upstream_chords;
+  o.downstream_chords = r.grid_downstream_chords;
+  o.vertical_chords = r.grid_vertical_chords;
+  char name[9] = {0};
+  std::memcpy(name, r.designation, 8);
+  if (cfd_status st = cfdb::makeCGrid(name, o, m.get()); st != CFD_OK) return st;
+  g.meshes[key] = m;
+  *out = m;
+  return CFD_OK;
+}
+
+}  // namespace
+
+cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* r, int* id) {
+  if (e == nullptr || r == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  if (cfd_status st = checkRequest(r); st != CFD_OK) return st;
+  cfdb::Engine& g = e->engine;
+  std::shared_ptr<const cfdb::HostMesh> mesh;
+  if (cfd_status st = meshFor(g, *r, &mesh); st != CFD_OK) return st;
   cfdb::Pending q;
   q.id = g.nextId++;
   q.request = *r;
@@ -504,6 +610,67 @@ cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* r, int* id) {
   q.submitted = g.now();
   g.queue.push_back(q);
   if (id != nullptr) *id = q.id;
+  return CFD_OK;
+}
+
+cfd_status cfd_sweep_angles(double start, double end, double step, double* out, int capacity, int* count) {
+  if (count == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null count");
+  if (!std::isfinite(start) || !std::isfinite(end) || !std::isfinite(step)) {
+    return cfdb::fail(CFD_INVALID_ARGUMENT, "sweep bounds must be finite");
+  }
+  if (!(step > 0.0)) return cfdb::fail(CFD_INVALID_ARGUMENT, "the sweep step must be positive");
+  // the step's sign comes from the direction of the sweep; the point count
+  // is rounded when the step divides the range to within 1e-9 of a step
+  const double signedStep = (end < start) ? -step : step;
+  const double span = (end - start) / signedStep;
+  const double rounded = std::round(span);
+  const double intervals = (std::abs(span - rounded) < 1e-9) ? rounded : std::floor(span);
+  if (intervals < 0.0) return cfdb::fail(CFD_INVALID_ARGUMENT, "the sweep covers no angles");
+  const double points = intervals + 1.0;
+  if (points > static_cast<double>(cfdb::kMaxSweepPoints)) {
+    char message[160];
+    std::snprintf(message, sizeof(message),
+                  "a sweep of %.0f points is more than the %d allowed; every point is a full solve",
+                  points, cfdb::kMaxSweepPoints);
+    return cfdb::fail(CFD_INVALID_ARGUMENT, message);
+  }
+  const int n = static_cast<int>(points);
+  *count = n;
+  if (out == nullptr) return CFD_OK;
+  if (capacity < n) return cfdb::fail(CFD_OUT_OF_RANGE, "angle buffer too small");
+  // each angle computed from its index, so a long sweep does not drift
+  for (int k = 0; k < n; ++k) out[k] = start + static_cast<double>(k) * signedStep;
+  return CFD_OK;
+}
+
+cfd_status cfd_engine_submit_sweep(cfd_engine e, const cfd_request* base, double start, double end,
+                                   double step, int continued, int* first_id, int* count) {
+  if (e == nullptr || base == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
+  if (cfd_status st = checkRequest(base); st != CFD_OK) return st;
+  int n = 0;
+  if (cfd_status st = cfd_sweep_angles(start, end, step, nullptr, 0, &n); st != CFD_OK) return st;
+  cfdb::Engine& g = e->engine;
+  cfdb::Sweep sw;
+  sw.base = *base;
+  sw.angles.resize(static_cast<std::size_t>(n));
+  if (cfd_status st = cfd_sweep_angles(start, end, step, sw.angles.data(), n, &n); st != CFD_OK) return st;
+  std::shared_ptr<const cfdb::HostMesh> mesh;
+  if (cfd_status st = meshFor(g, *base, &mesh); st != CFD_OK) return st;
+  sw.firstId = g.nextId;
+  sw.continued = (continued != 0);
+  g.nextId += n;
+  cfdb::Pending q;
+  q.id = sw.firstId;
+  q.request = *base;
+  q.request.alpha_deg = sw.angles.front();
+  q.mesh = mesh;
+  q.submitted = g.now();
+  q.sweep = static_cast<int>(g.sweeps.size());
+  q.point = 0;
+  g.sweeps.push_back(std::move(sw));
+  g.queue.push_back(q);
+  if (first_id != nullptr) *first_id = q.id;
+  if (count != nullptr) *count = n;
   return CFD_OK;
 }
 

@@ -54,6 +54,7 @@ enum Stage : int {
 constexpr int kFlagGlobalCg = 1;
 constexpr int kFlagPlainWavefront = 2;
 constexpr int kFlagSequentialRows = 4;
+constexpr int kFlagTwoReductionCg = 8;
 
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {
@@ -131,9 +132,10 @@ struct Instance {
   double *gux, *guy, *gvx, *gvy, *gpx, *gpy;
   // momentum system (shared by u and v), relaxed; aD doubles as momentumDiagonal
   double *aD, *aS, *aN, *aW, *aE, *bU, *bV;
-  // pressure correction
+  // pressure correction; the single-reduction CG double-buffers r in (r, z),
+  // w = A u in (q, d0) and s = A p in (d1, s1), with the direction in cgp
   double *pD, *pN, *pE, *pB, *net;
-  double *x, *r, *z, *q, *d0, *d1;
+  double *x, *r, *z, *q, *d0, *d1, *s1, *cgp;
   double* div;
 
   // ---- SST ----

@@ -1050,115 +1050,328 @@ DEV void phaseSstFinish(const Instance& I, Team& t, double (&mx)[8]) {
   }
 }
 
-// ---- pressure CG with the band in shared memory -----------------------------------
+// ---- pressure CG: one reduction per iteration ----------------------------------
+//
+// The reference's Jacobi-PCG (LinearSystem.cpp:118-210) needs two global
+// reductions per iteration (d.Ad, then r.z and sum |r|): two cluster barriers.
+// Here it is rearranged as Chronopoulos and Gear's single-reduction PCG
+// (J. Comput. Appl. Math. 25, 1989), which computes the same iterates in
+// exact arithmetic with one reduction of three sums per iteration:
+//
+//   u = M^-1 r,  w = A u,  gamma = r.u,  delta = w.u,  rho = sum |r|
+//   beta_k = gamma_k / gamma_(k-1),  d.Ad_k = delta_k - beta_k gamma_k / alpha_(k-1),
+//   alpha_k = gamma_k / d.Ad_k
+//   p = u + beta p,  s = w + beta s (= A p),  x += alpha p,  r -= alpha s
+//
+// with the reference's stopping rule (rho <= tolerance * rho_0, tested after
+// each update), its cap, and its breakdown guards (d.Ad = 0 before an update,
+// r.z = 0 before forming beta). One launch phase per iteration: each cell
+// forms its own p, s, x, r and u' = M^-1 r', and w' = A u' from its
+// neighbours' u', which it recomputes from their r, w and s of the previous
+// iteration (read from the other half of double-buffered r, w and s, so no
+// neighbour's update can race with the read). Every cell's u' is the same
+// expression in every thread that forms it, so the bits agree.
+//
+// Rounding: the iterates differ from the reference's two-reduction form only
+// in the last bits (~1e-13 relative after 200 iterations on the 384x96 and
+// 768x192 pressure systems, the same order as summing the dot products in
+// another order), checked by the parity tests after the pressure solve.
 
-/// Shared-memory CG layout: 11 arrays of `stride` doubles per CTA, where
-/// stride = ceil(NJ / R) * NI is the largest band of rows any rank holds, so
-/// every CTA lays its arrays out identically and a neighbour's value is found
-/// at the same offset through DSMEM.
-enum CgSmemArray : int { kSD = 0, kSS, kSN, kSW, kSE, kSX, kSR, kSZ, kSQ, kSD0, kSD1, kCgArrays };
+DEV double precondition(double rc, double dg) { return (fabs(dg) > 0.0) ? rc / dg : rc; }
 
-__host__ __device__ inline int cgSmemStride(int NI, int NJ, int R) { return ((NJ + R - 1) / R) * NI; }
-
-/// Where cell n lives during the shared-memory CG: this CTA's band, or the
-/// band just below or just above it (the only other rows a 5-point stencil
-/// reaches; the wake partner of a row-0 cell is in row 0).
-struct Band {
-  int c0, c1, NI, NJ, R, rank;
-  int cBelow, cAbove;  // first cell of the neighbouring bands
+/// The three reduced sums of one iteration, and the scalars they give.
+struct CgScalars {
+  double alpha{0.0}, beta{0.0}, gamma{0.0};
 };
+
+/// After a reduction of {gamma', delta', rho'}: the reference's stop tests and
+/// the next alpha and beta. Returns false when the solve stops.
+DEV bool cgNext(const Instance& I, CgScalars& k, const double (&acc)[3], double initial) {
+  if (acc[2] <= I.cgTol * initial) return false;  // converged
+  if (!(fabs(k.gamma) > 0.0)) return false;        // r.z vanished
+  const double beta = acc[0] / k.gamma;
+  const double dAd = acc[1] - beta * acc[0] / k.alpha;  // p.Ap of the next direction
+  if (!(fabs(dAd) > 0.0)) return false;
+  k.beta = beta;
+  k.alpha = acc[0] / dAd;
+  k.gamma = acc[0];
+  return true;
+}
+
+/// Band layout of the shared-memory CG: per CTA, 9 cell arrays of `stride`
+/// doubles (stride = the largest band's cells, so a neighbour's value sits at
+/// the same offset in its CTA) and the band's face coefficients: north-family
+/// faces of rows j0 .. j1 (stride + NI) and east-family faces (stride + rows).
+enum CgSmemArray : int { kSD = 0, kSX, kSP, kSR0, kSR1, kSW0, kSW1, kSS0, kSS1, kCgCellArrays };
+
+__host__ __device__ inline int cgRowsMax(int NJ, int R) { return (NJ + R - 1) / R; }
+__host__ __device__ inline int cgSmemStride(int NI, int NJ, int R) { return cgRowsMax(NJ, R) * NI; }
+__host__ __device__ inline long long cgSmemDoubles(int NI, int NJ, int R) {
+  const long long stride = cgSmemStride(NI, NJ, R);
+  return kCgCellArrays * stride + (stride + NI) + (stride + cgRowsMax(NJ, R));
+}
 
 DEV int bandFirstCell(int NI, int NJ, int R, int r) { return NI * ((NJ * r) / R); }
 
-/// Jacobi-PCG identical in arithmetic, cell order and reduction order to the
-/// global-memory loop; the vectors and rows of the band stay in shared
-/// memory and the halo rows are read from the neighbouring CTAs. Returns the
-/// iterations run; x is written back to global memory at the end.
-DEV int cgShared(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double rz) {
-  const int stride = cgSmemStride(I.NI, I.NJ, static_cast<int>(t.R));
-  double* a[kCgArrays];
-#pragma unroll
-  for (int k = 0; k < kCgArrays; ++k) a[k] = dyn + k * stride;
+/// The single-reduction PCG with the band in shared memory: vectors, the
+/// diagonal and the face coefficients stay on chip; a neighbour in the band
+/// below or above is read from that CTA's shared memory (DSMEM). On entry
+/// I.r = b (x = 0); `initial` = sum |b|, `gamma` = b.M^-1 b. Returns the
+/// iterations run; x is written to global memory at the end.
+DEV int cgShared(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double gamma) {
   const int NI = I.NI, NJ = I.NJ;
   const int R = static_cast<int>(t.R), rank = static_cast<int>(t.rank);
+  const int stride = cgSmemStride(NI, NJ, R);
+  double* a[kCgCellArrays];
+#pragma unroll
+  for (int k = 0; k < kCgCellArrays; ++k) a[k] = dyn + k * stride;
+  double* fN = dyn + kCgCellArrays * stride;  // face row j0 + lj at lj * NI
+  double* fE = fN + stride + NI;              // row j0 + lj at lj * (NI + 1)
+  const int j0 = t.c0 / NI;
   const int cBelow = (rank > 0) ? bandFirstCell(NI, NJ, R, rank - 1) : 0;
-  const int cAbove = t.c1;  // the band above starts where this one ends
-  // Remote (DSMEM) views of the neighbouring bands' z, d0 and d1.
-  const double* zB = (rank > 0) ? t.cl.map_shared_rank(a[kSZ], rank - 1) : nullptr;
-  const double* dB0 = (rank > 0) ? t.cl.map_shared_rank(a[kSD0], rank - 1) : nullptr;
-  const double* dB1 = (rank > 0) ? t.cl.map_shared_rank(a[kSD1], rank - 1) : nullptr;
-  const double* zA = (rank < R - 1) ? t.cl.map_shared_rank(a[kSZ], rank + 1) : nullptr;
-  const double* dA0 = (rank < R - 1) ? t.cl.map_shared_rank(a[kSD0], rank + 1) : nullptr;
-  const double* dA1 = (rank < R - 1) ? t.cl.map_shared_rank(a[kSD1], rank + 1) : nullptr;
-
+  const int cAbove = t.c1;
+  // remote views of the neighbouring bands' diagonal, r, w and s
+  double* below[kCgCellArrays] = {};
+  double* above[kCgCellArrays] = {};
+#pragma unroll
+  for (int k = 0; k < kCgCellArrays; ++k) {
+    if (rank > 0) below[k] = t.cl.map_shared_rank(a[k], rank - 1);
+    if (rank < R - 1) above[k] = t.cl.map_shared_rank(a[k], rank + 1);
+  }
+  // load the band: diagonal, b, zero x, p and s; the face coefficients with
+  // the boundary faces' zeros (the wake cut's j = 0 faces keep theirs)
   for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-    const int k = c - t.c0;
-    const int i = c % NI, j = c / NI;
-    a[kSD][k] = I.pD[c];
-    a[kSS][k] = (j > 0) ? I.pN[j * NI + i] : ((I.acrossJ0[i] >= 0) ? I.pN[i] : 0.0);
-    a[kSN][k] = (j < NJ - 1) ? I.pN[(j + 1) * NI + i] : 0.0;
-    a[kSW][k] = (i > 0) ? I.pE[j * (NI + 1) + i] : 0.0;
-    a[kSE][k] = (i < NI - 1) ? I.pE[j * (NI + 1) + i + 1] : 0.0;
-    a[kSX][k] = 0.0;
-    a[kSR][k] = I.r[c];
-    a[kSZ][k] = I.z[c];
-    a[kSD0][k] = I.d0[c];
+    const int m = c - t.c0;
+    a[kSD][m] = I.pD[c];
+    a[kSX][m] = 0.0;
+    a[kSP][m] = 0.0;
+    a[kSR0][m] = I.r[c];
+    a[kSS0][m] = 0.0;
+  }
+  const int rows = (t.c1 - t.c0) / NI;
+  for (int k = t.tid; k < (rows + 1) * NI; k += t.T) {
+    const int lj = k / NI, i = k % NI, j = j0 + lj;
+    double v = 0.0;
+    if (j > 0 && j < NJ) v = I.pN[j * NI + i];
+    else if (j == 0 && I.acrossJ0[i] >= 0) v = I.pN[i];
+    fN[k] = v;
+  }
+  for (int k = t.tid; k < rows * (NI + 1); k += t.T) {
+    const int lj = k / (NI + 1), i = k % (NI + 1), j = j0 + lj;
+    fE[k] = (i > 0 && i < NI) ? I.pE[j * (NI + 1) + i] : 0.0;
   }
   t.cl.sync();  // every band loaded before anyone reads a neighbour's
 
-  int cgIters = 0;
-  double beta = 0.0;
-  int cur = 0;  // which d buffer holds the current direction (0: d0, 1: d1)
-  const int op1[1] = {kSum};
-  const int op2[2] = {kSum, kSum};
-  for (int iter = 0; iter < I.cgMax; ++iter) {
-    double* dCur = a[cur ? kSD1 : kSD0];
-    double* dNext = a[cur ? kSD0 : kSD1];
-    const double* dBc = cur ? dB1 : dB0;
-    const double* dAc = cur ? dA1 : dA0;
-    double dAd[1] = {0.0};
+  // where cell n's array k lives: this band, the band below, or above
+  auto at = [&](int k, int n) -> double {
+    if (n >= t.c0 && n < t.c1) return a[k][n - t.c0];
+    if (n < t.c0) return below[k][n - cBelow];
+    return above[k][n - cAbove];
+  };
+  // w0 = A u0 and delta0 = w0.u0
+  {
+    double acc[1] = {0.0};
+    const int op1[1] = {kSum};
     for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-      const int k = c - t.c0;
-      const int i = c % NI, j = c / NI;
-      // value of the direction at cell n: d itself on the first iteration,
-      // z + beta d afterwards; n in this band, or in the band below/above
-      auto dirAt = [&](int n) -> double {
-        if (n >= t.c0 && n < t.c1) {
-          const int m = n - t.c0;
-          return (iter == 0) ? dCur[m] : a[kSZ][m] + beta * dCur[m];
-        }
-        if (n < t.c0) {
-          const int m = n - cBelow;
-          return (iter == 0) ? dBc[m] : zB[m] + beta * dBc[m];
-        }
-        const int m = n - cAbove;
-        return (iter == 0) ? dAc[m] : zA[m] + beta * dAc[m];
-      };
-      const double dc = (iter == 0) ? dCur[k] : a[kSZ][k] + beta * dCur[k];
-      if (iter > 0) dNext[k] = dc;
-      double y = a[kSD][k] * dc;
-      int n = (j > 0) ? c - NI : I.acrossJ0[i];
-      if (n >= 0) y += a[kSS][k] * dirAt(n);
-      if (j < NJ - 1) y += a[kSN][k] * dirAt(c + NI);
-      if (i > 0) y += a[kSW][k] * dirAt(c - 1);
-      if (i < NI - 1) y += a[kSE][k] * dirAt(c + 1);
-      a[kSQ][k] = y;
-      dAd[0] += dc * y;
+      const int m = c - t.c0, i = c % NI, j = c / NI, lj = j - j0;
+      auto uAt = [&](int n) { return precondition(at(kSR0, n), at(kSD, n)); };
+      const double un = precondition(a[kSR0][m], a[kSD][m]);
+      double y = a[kSD][m] * un;
+      const int nS = (j > 0) ? c - NI : I.acrossJ0[i];
+      if (nS >= 0) y += fN[lj * NI + i] * uAt(nS);
+      if (j < NJ - 1) y += fN[(lj + 1) * NI + i] * uAt(c + NI);
+      if (i > 0) y += fE[lj * (NI + 1) + i] * uAt(c - 1);
+      if (i < NI - 1) y += fE[lj * (NI + 1) + i + 1] * uAt(c + 1);
+      a[kSW0][m] = y;
+      acc[0] += y * un;
     }
-    if (iter > 0) cur ^= 1;
-    teamReduce(t, sh, dAd, op1);
+    teamReduce(t, sh, acc, op1);
+    if (!(fabs(acc[0]) > 0.0)) {
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] = 0.0;
+      t.cl.sync();
+      return 0;
+    }
+    CgScalars k0;
+    k0.alpha = gamma / acc[0];
+    k0.gamma = gamma;
+    int iterations = 0;
+    int cur = 0;
+    const int op3[3] = {kSum, kSum, kSum};
+    CgScalars k = k0;
+    for (int iter = 0; iter < I.cgMax; ++iter) {
+      const int rC = cur ? kSR1 : kSR0, rN = cur ? kSR0 : kSR1;
+      const int wC = cur ? kSW1 : kSW0, wN = cur ? kSW0 : kSW1;
+      const int sC = cur ? kSS1 : kSS0, sN = cur ? kSS0 : kSS1;
+      const double alpha = k.alpha, beta = k.beta;
+      double sums[3] = {0.0, 0.0, 0.0};
+      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+        const int m = c - t.c0, i = c % NI, j = c / NI, lj = j - j0;
+        // the next u of a cell from its r, w and s of this iteration
+        auto uAt = [&](int n) {
+          const double sn = at(wC, n) + beta * at(sC, n);
+          return precondition(at(rC, n) - alpha * sn, at(kSD, n));
+        };
+        const double dg = a[kSD][m];
+        const double pc = precondition(a[rC][m], dg) + beta * a[kSP][m];
+        const double sc = a[wC][m] + beta * a[sC][m];
+        a[kSX][m] += alpha * pc;
+        const double rc = a[rC][m] - alpha * sc;
+        const double un = precondition(rc, dg);
+        double y = dg * un;
+        const int nS = (j > 0) ? c - NI : I.acrossJ0[i];
+        if (nS >= 0) y += fN[lj * NI + i] * uAt(nS);
+        if (j < NJ - 1) y += fN[(lj + 1) * NI + i] * uAt(c + NI);
+        if (i > 0) y += fE[lj * (NI + 1) + i] * uAt(c - 1);
+        if (i < NI - 1) y += fE[lj * (NI + 1) + i + 1] * uAt(c + 1);
+        a[kSP][m] = pc;
+        a[sN][m] = sc;
+        a[rN][m] = rc;
+        a[wN][m] = y;
+        sums[0] += rc * un;
+        sums[1] += y * un;
+        sums[2] += fabs(rc);
+      }
+      cur ^= 1;
+      teamReduce(t, sh, sums, op3);
+      iterations = iter + 1;
+      if (!cgNext(I, k, sums, initial)) break;
+    }
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] = a[kSX][c - t.c0];
+    t.cl.sync();  // x visible to the correction; no peer still reads this band
+    return iterations;
+  }
+}
+
+/// The same single-reduction PCG with the vectors in global memory (bands
+/// too large for shared memory): x, p, and r, w, s double-buffered as
+/// (r, z), (q, d0), (d1, s1). Same arithmetic, cell order and reduction
+/// order as cgShared, so both give the same bits.
+DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double gamma) {
+  const int NI = I.NI, NJ = I.NJ;
+  double* rB[2] = {I.r, I.z};
+  double* wB[2] = {I.q, I.d0};
+  double* sB[2] = {I.d1, I.s1};
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    I.cgp[c] = 0.0;
+    sB[0][c] = 0.0;
+  }
+  // w0 = A u0 (u0 from b, stable since the start's reduction)
+  double acc[1] = {0.0};
+  const int op1[1] = {kSum};
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % NI, j = c / NI;
+    auto uAt = [&](int n) { return precondition(rB[0][n], I.pD[n]); };
+    const double un = precondition(rB[0][c], I.pD[c]);
+    double y = I.pD[c] * un;
+    const int nS = (j > 0) ? c - NI : I.acrossJ0[i];
+    if (nS >= 0) y += I.pN[j * NI + i] * uAt(nS);
+    if (j < NJ - 1) y += I.pN[(j + 1) * NI + i] * uAt(c + NI);
+    if (i > 0) y += I.pE[j * (NI + 1) + i] * uAt(c - 1);
+    if (i < NI - 1) y += I.pE[j * (NI + 1) + i + 1] * uAt(c + 1);
+    wB[0][c] = y;
+    acc[0] += y * un;
+  }
+  teamReduce(t, sh, acc, op1);
+  if (!(fabs(acc[0]) > 0.0)) return 0;
+  CgScalars k;
+  k.alpha = gamma / acc[0];
+  k.gamma = gamma;
+  int iterations = 0;
+  int cur = 0;
+  const int op3[3] = {kSum, kSum, kSum};
+  for (int iter = 0; iter < I.cgMax; ++iter) {
+    const double* __restrict__ r = rB[cur];
+    const double* __restrict__ w = wB[cur];
+    const double* __restrict__ sv = sB[cur];
+    double* __restrict__ rn = rB[cur ^ 1];
+    double* __restrict__ wn = wB[cur ^ 1];
+    double* __restrict__ sn = sB[cur ^ 1];
+    const double alpha = k.alpha, beta = k.beta;
+    double sums[3] = {0.0, 0.0, 0.0};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % NI, j = c / NI;
+      auto uAt = [&](int n) {
+        const double s2 = w[n] + beta * sv[n];
+        return precondition(r[n] - alpha * s2, I.pD[n]);
+      };
+      const double dg = I.pD[c];
+      const double pc = precondition(r[c], dg) + beta * I.cgp[c];
+      const double sc = w[c] + beta * sv[c];
+      I.x[c] += alpha * pc;
+      const double rc = r[c] - alpha * sc;
+      const double un = precondition(rc, dg);
+      double y = dg * un;
+      const int nS = (j > 0) ? c - NI : I.acrossJ0[i];
+      if (nS >= 0) y += I.pN[j * NI + i] * uAt(nS);
+      if (j < NJ - 1) y += I.pN[(j + 1) * NI + i] * uAt(c + NI);
+      if (i > 0) y += I.pE[j * (NI + 1) + i] * uAt(c - 1);
+      if (i < NI - 1) y += I.pE[j * (NI + 1) + i + 1] * uAt(c + 1);
+      I.cgp[c] = pc;
+      sn[c] = sc;
+      rn[c] = rc;
+      wn[c] = y;
+      sums[0] += rc * un;
+      sums[1] += y * un;
+      sums[2] += fabs(rc);
+    }
+    cur ^= 1;
+    teamReduce(t, sh, sums, op3);
+    iterations = iter + 1;
+    if (!cgNext(I, k, sums, initial)) break;
+  }
+  return iterations;
+}
+
+/// The reference's two-reduction Jacobi-PCG with the vectors in global memory
+/// (kernel flag bit 3; kept to compare with): the next direction d' = z +
+/// beta d is formed redundantly for each neighbour from z and d, which are
+/// both stable across the barrier, so A d' needs no extra exchange.
+DEV int cgTwoReductions(const Instance& I, Team& t, Shared& sh, double initial, double rz) {
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const double zc = precondition(I.r[c], I.pD[c]);
+    I.z[c] = zc;
+    I.d0[c] = zc;
+  }
+  t.cl.sync();
+  const int op2[2] = {kSum, kSum};
+  int cgIters = 0;
+  double* dCur = I.d0;
+  double* dNext = I.d1;
+  double beta = 0.0;
+  for (int iter = 0; iter < I.cgMax; ++iter) {
+    double dAd[1] = {0.0};
+    const int opS[1] = {kSum};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % I.NI, j = c / I.NI;
+      double dc;
+      if (iter == 0) {
+        dc = dCur[c];
+        I.q[c] = pressureRow(I, c, i, j, dCur, dc);
+      } else {
+        dc = I.z[c] + beta * dCur[c];
+        dNext[c] = dc;
+        double y = I.pD[c] * dc;
+        int n = (j > 0) ? c - I.NI : I.acrossJ0[i];
+        if (n >= 0) y += I.pN[j * I.NI + i] * (I.z[n] + beta * dCur[n]);
+        if (j < I.NJ - 1) { n = c + I.NI; y += I.pN[(j + 1) * I.NI + i] * (I.z[n] + beta * dCur[n]); }
+        if (i > 0) { n = c - 1; y += I.pE[j * (I.NI + 1) + i] * (I.z[n] + beta * dCur[n]); }
+        if (i < I.NI - 1) { n = c + 1; y += I.pE[j * (I.NI + 1) + i + 1] * (I.z[n] + beta * dCur[n]); }
+        I.q[c] = y;
+      }
+      dAd[0] += dc * I.q[c];
+    }
+    if (iter > 0) { double* tmp = dCur; dCur = dNext; dNext = tmp; }
+    teamReduce(t, sh, dAd, opS);
     if (!(fabs(dAd[0]) > 0.0)) break;
     const double step = rz / dAd[0];
-    double* dNow = a[cur ? kSD1 : kSD0];
     double rr[2] = {0.0, 0.0};
     for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-      const int k = c - t.c0;
-      a[kSX][k] += step * dNow[k];
-      const double rc = a[kSR][k] - step * a[kSQ][k];
-      a[kSR][k] = rc;
-      const double dg = a[kSD][k];
-      const double zc = (fabs(dg) > 0.0) ? rc / dg : rc;
-      a[kSZ][k] = zc;
+      const double dc = dCur[c];
+      I.x[c] += step * dc;
+      const double rc = I.r[c] - step * I.q[c];
+      I.r[c] = rc;
+      const double zc = precondition(rc, I.pD[c]);
+      I.z[c] = zc;
       rr[0] += fabs(rc);
       rr[1] += rc * zc;
     }
@@ -1169,8 +1382,6 @@ DEV int cgShared(const Instance& I, Team& t, Shared& sh, double* dyn, double ini
     beta = rr[1] / rz;
     rz = rr[1];
   }
-  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) I.x[c] = a[kSX][c - t.c0];
-  t.cl.sync();  // x visible to the correction; no peer still reads this band
   return cgIters;
 }
 
@@ -1199,10 +1410,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
   t.c1 = I.NI * ((I.NJ * (static_cast<int>(t.rank) + 1)) / static_cast<int>(t.R));
   const bool sst = (I.model == 2);
   // The pressure CG keeps its band in shared memory when every band has a
-  // row and the largest band's 11 arrays fit in what the launch provides.
-  const bool cgInShared =
-      !(flags & kFlagGlobalCg) && I.NJ >= static_cast<int>(t.R) &&
-      static_cast<long long>(kCgArrays) * cgSmemStride(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
+  // row and the largest band's arrays fit in what the launch provides.
+  const bool cgInShared = !(flags & (kFlagGlobalCg | kFlagTwoReductionCg)) && I.NJ >= static_cast<int>(t.R) &&
+                          cgSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
   const bool leader = (t.rank == 0 && t.tid == 0);
 
   int done = 0;
@@ -1275,79 +1485,28 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
         double b = I.pB[c];
         if (!I.hasPRef) { b -= mean; I.pB[c] = b; }
-        const double dg = I.pD[c];
-        const double zc = (fabs(dg) > 0.0) ? b / dg : b;
         I.x[c] = 0.0;
         I.r[c] = b;
-        I.z[c] = zc;
-        I.d0[c] = zc;
         init[0] += fabs(b);
-        init[1] += b * zc;
+        init[1] += b * precondition(b, I.pD[c]);
       }
       teamReduce(t, sh, init, op2);
       if (stopStage == kStagePressureAssembly) { stopped = true; break; }
 
-      // 6. Jacobi-preconditioned CG (LinearSystem.cpp:118-210), two cluster
-      // barriers per iteration: the next direction d' = z + beta d is formed
-      // redundantly for each neighbour from z and d, which are both stable
-      // across the barrier, so A d' needs no extra exchange.
+      // 6. the pressure correction: Jacobi-preconditioned CG (LinearSystem.cpp:
+      // 118-210) with one reduction per iteration (cgShared / cgGlobal), or
+      // the mixed form's multigrid CG.
       const double initial = init[0];
-      double rz = init[1];
+      const double rz = init[1];
       int cgIters = 0;
       if (initial > 0.0 && I.precision == 1) {
         cgIters = pressureMixed(I, t, sh, dyn, initial);
+      } else if (initial > 0.0 && (flags & kFlagTwoReductionCg)) {
+        cgIters = cgTwoReductions(I, t, sh, initial, rz);
       } else if (initial > 0.0 && cgInShared) {
         cgIters = cgShared(I, t, sh, dyn, initial, rz);
       } else if (initial > 0.0) {
-        double* dCur = I.d0;
-        double* dNext = I.d1;
-        double beta = 0.0;
-        for (int iter = 0; iter < I.cgMax; ++iter) {
-          double dAd[1] = {0.0};
-          const int opS[1] = {kSum};
-          for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-            const int i = c % I.NI, j = c / I.NI;
-            double dc;
-            if (iter == 0) {
-              dc = dCur[c];
-              I.q[c] = pressureRow(I, c, i, j, dCur, dc);
-            } else {
-              // d' for this cell and its neighbours, then A d'.
-              dc = I.z[c] + beta * dCur[c];
-              dNext[c] = dc;
-              double y = I.pD[c] * dc;
-              int n = (j > 0) ? c - I.NI : I.acrossJ0[i];
-              if (n >= 0) y += I.pN[j * I.NI + i] * (I.z[n] + beta * dCur[n]);
-              if (j < I.NJ - 1) { n = c + I.NI; y += I.pN[(j + 1) * I.NI + i] * (I.z[n] + beta * dCur[n]); }
-              if (i > 0) { n = c - 1; y += I.pE[j * (I.NI + 1) + i] * (I.z[n] + beta * dCur[n]); }
-              if (i < I.NI - 1) { n = c + 1; y += I.pE[j * (I.NI + 1) + i + 1] * (I.z[n] + beta * dCur[n]); }
-              I.q[c] = y;
-            }
-            dAd[0] += dc * I.q[c];
-          }
-          if (iter > 0) { double* tmp = dCur; dCur = dNext; dNext = tmp; }
-          teamReduce(t, sh, dAd, opS);
-          if (!(fabs(dAd[0]) > 0.0)) break;
-          const double step = rz / dAd[0];
-          double rr[2] = {0.0, 0.0};
-          for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-            const double dc = dCur[c];
-            I.x[c] += step * dc;
-            const double rc = I.r[c] - step * I.q[c];
-            I.r[c] = rc;
-            const double dg = I.pD[c];
-            const double zc = (fabs(dg) > 0.0) ? rc / dg : rc;
-            I.z[c] = zc;
-            rr[0] += fabs(rc);
-            rr[1] += rc * zc;
-          }
-          teamReduce(t, sh, rr, op2);
-          cgIters = iter + 1;
-          if (rr[0] <= I.cgTol * initial) break;
-          if (!(fabs(rz) > 0.0)) break;
-          beta = rr[1] / rz;
-          rz = rr[1];
-        }
+        cgIters = cgGlobal(I, t, sh, initial, rz);
       }
       mon[kMonPressureIterations] += static_cast<double>(cgIters);
       if (!I.hasPRef) {
@@ -1504,10 +1663,12 @@ int chooseClusterSize(int cells) {
 }
 
 int kernelFlags() {
-  // Implementation choices for tuning comparisons (results are identical):
-  // bit 0 keeps the pressure CG in global memory, bit 1 uses the plain
-  // wavefront sweeps, bit 2 runs the k/omega row sweeps one after another
-  // instead of pipelined across CTAs.
+  // Implementation choices for tuning comparisons: bit 0 keeps the pressure
+  // CG in global memory, bit 1 uses the plain wavefront sweeps, bit 2 runs
+  // the k/omega row sweeps one after another instead of pipelined across
+  // CTAs (these three give identical results); bit 3 runs the reference's
+  // two-reduction CG instead of the single-reduction one (the same to
+  // rounding).
   const char* env = std::getenv("CFD_KERNEL_FLAGS");
   return (env != nullptr) ? std::atoi(env) : 0;
 }
@@ -1516,7 +1677,7 @@ int cgSharedBytes(int NI, int NJ, int clusterSize) {
   // The k/omega row sweeps keep two rows and the scan's warp totals.
   const long long wave = (2LL * NI + 64) * 8;
   long long bytes = 0;
-  if (NJ >= clusterSize) bytes = static_cast<long long>(kCgArrays) * cgSmemStride(NI, NJ, clusterSize) * 8;
+  if (NJ >= clusterSize) bytes = cgSmemDoubles(NI, NJ, clusterSize) * 8;
   if (bytes > kMaxCgSharedBytes) bytes = 0;
   if (bytes < wave && wave <= kMaxCgSharedBytes) bytes = wave;
   return static_cast<int>(bytes);

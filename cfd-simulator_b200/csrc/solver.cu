@@ -312,7 +312,7 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     I.wallMask = a.take<uint8_t>(N);
     double** cellArrays[] = {&I.u, &I.v, &I.p, &I.rho, &I.mu, &I.muMol, &I.gux, &I.guy, &I.gvx,
                              &I.gvy, &I.gpx, &I.gpy, &I.aD, &I.aS, &I.aN, &I.aW, &I.aE, &I.bU,
-                             &I.bV, &I.pD, &I.pB, &I.net, &I.x, &I.r, &I.z, &I.q, &I.d0, &I.d1,
+                             &I.bV, &I.pD, &I.pB, &I.net, &I.x, &I.r, &I.z, &I.q, &I.d0, &I.d1, &I.s1, &I.cgp,
                              &I.div, &I.k, &I.om, &I.mut, &I.strain, &I.f1, &I.f2, &I.cd, &I.prod,
                              &I.gkx, &I.gky, &I.gwx, &I.gwy, &I.kD, &I.kS, &I.kN, &I.kW, &I.kE,
                              &I.kB, &I.wD, &I.wS, &I.wN, &I.wW, &I.wE, &I.wB};

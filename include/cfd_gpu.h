@@ -287,7 +287,11 @@ typedef struct cfd_request {
   cfd_settings settings;
 } cfd_request;
 
-enum { CFD_SOLVE_CONVERGED = 0, CFD_SOLVE_ITERATION_LIMIT = 1, CFD_SOLVE_DIVERGED = 2 };
+/* Outcomes (pointStatus, Polar.cpp:79-84), plus a request that never started
+ * because its solver could not be built or initialised (cfd_result.error
+ * then holds the library's status code). */
+enum { CFD_SOLVE_CONVERGED = 0, CFD_SOLVE_ITERATION_LIMIT = 1, CFD_SOLVE_DIVERGED = 2,
+       CFD_SOLVE_FAILED = 3 };
 
 typedef struct cfd_result {
   int id;
@@ -301,6 +305,9 @@ typedef struct cfd_result {
   double pressure_drag_coefficient, friction_drag_coefficient;
   double submitted_s, started_s, finished_s;  /* engine clock, seconds */
   double separation_upper_chord_fraction, separation_lower_chord_fraction;  /* or -1 */
+  double alpha_deg;              /* the incidence solved (a sweep's points get theirs here) */
+  int continued;                 /* 1: started from the previous sweep point's u and p */
+  int error;                     /* CFD_SOLVE_FAILED: why the solve could not start */
 } cfd_result;
 
 /* memory_budget_bytes: device memory the resident solves may hold (0: 80 %
@@ -312,6 +319,25 @@ cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* request, int* id);
  * iterations, retire finished ones. active/queued (may be NULL) report the
  * counts afterwards. */
 cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued);
+/* post::sweepAngles (src/post/Polar.cpp:36-77): the angles from start to end
+ * (a descending sweep when end < start) in steps of |step|, the point count
+ * rounded when the step divides the range, at most 400 points; the
+ * reference's refusals (non-finite bounds, step <= 0, an empty or too long
+ * sweep) return CFD_INVALID_ARGUMENT with its message. out may be NULL to
+ * query *count. */
+cfd_status cfd_sweep_angles(double start, double end, double step, double* out, int capacity,
+                            int* count);
+/* A polar sweep as the reference runs one (startPolarSweep / updatePolar,
+ * src/app/Panels.cpp:1601-1797): one solve of `base` per angle of
+ * cfd_sweep_angles(start, end, step), each started when the previous point
+ * has retired. continued = 1 starts every point after the first from the
+ * previous point's u and p (k and omega from their freestream and wall seeds,
+ * as Panels.cpp:1145-1156 rebuilds the solver), except after a point that
+ * diverged even on its cold retry. The points get the ids first_id ..
+ * first_id + count - 1 in sweep order; many sweeps (and single requests)
+ * share the GPU. */
+cfd_status cfd_engine_submit_sweep(cfd_engine e, const cfd_request* base, double start, double end,
+                                   double step, int continued, int* first_id, int* count);
 /* Move up to `capacity` finished results into `out`; *count gets how many. */
 cfd_status cfd_engine_results(cfd_engine e, cfd_result* out, int capacity, int* count);
 /* Launch shapes of the solves the engine starts from now on: 0 (default) by

@@ -46,6 +46,7 @@
 #include "cfd/mesh/CGrid.hpp"
 #include "cfd/mesh/Mesh.hpp"
 #include "cfd/post/Forces.hpp"
+#include "cfd/post/Polar.hpp"
 #include "cfd/post/SurfaceData.hpp"
 #include "cfd/solver/Gradient.hpp"
 #include "cfd/solver/KOmegaSST.hpp"
@@ -618,6 +619,61 @@ int ref_forces(void* s, double speed, double alphaDeg, double density, double re
     for (const auto& point : surface.value().lower) cp[k++] = point.pressureCoefficient;
   }
   return 0;
+}
+
+// ----------------------------------------------------------------- polar ---
+
+/// post::sweepAngles (Polar.cpp:36-77): the angle count, written to `out`
+/// when it has room; -1 on the reference's refusal (message in
+/// ref_last_error).
+int ref_sweep_angles(double start, double end, double step, double* out, int capacity) {
+  auto angles = cfd::post::sweepAngles(start, end, step);
+  if (!angles) {
+    g_error = angles.error().message();
+    return -1;
+  }
+  const auto& a = angles.value();
+  for (std::size_t k = 0; k < a.size() && static_cast<int>(k) < capacity; ++k) out[k] = a[k];
+  return static_cast<int>(a.size());
+}
+
+/// post::toCsv (Polar.cpp:126-164) of a polar given point by point: 13
+/// doubles per point {alpha, cl, cd, cd_pressure, cd_friction, cm, l_over_d,
+/// upper separation, lower separation, converged, diverged, iterations,
+/// continuity residual}. Returns the text's length; writes it (not
+/// terminated) when it fits `capacity`.
+int ref_polar_csv(const char* section, const char* mesh, double reynolds, double speed, double chord,
+                  double momentReference, int continued, int n, const double* points, char* out,
+                  int capacity) {
+  cfd::post::Polar polar;
+  polar.section = section;
+  polar.meshResolution = mesh;
+  polar.reynoldsNumber = reynolds;
+  polar.machEquivalentSpeed = speed;
+  polar.chord = chord;
+  polar.momentReferenceFraction = momentReference;
+  polar.continuedBetweenPoints = continued != 0;
+  for (int k = 0; k < n; ++k) {
+    const double* v = points + 13 * k;
+    cfd::post::PolarPoint p;
+    p.angleOfAttackDeg = v[0];
+    p.liftCoefficient = v[1];
+    p.dragCoefficient = v[2];
+    p.pressureDragCoefficient = v[3];
+    p.frictionDragCoefficient = v[4];
+    p.momentCoefficient = v[5];
+    p.liftToDrag = v[6];
+    p.upperSeparation = v[7];
+    p.lowerSeparation = v[8];
+    p.converged = v[9] != 0.0;
+    p.diverged = v[10] != 0.0;
+    p.iterations = static_cast<long long>(v[11]);
+    p.continuityResidual = v[12];
+    polar.points.push_back(p);
+  }
+  const std::string text = cfd::post::toCsv(polar);
+  if (static_cast<int>(text.size()) <= capacity) std::memcpy(out, text.data(), text.size());
+  return static_cast<int>(text.size());
 }
 
 }  // extern "C"

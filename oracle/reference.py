@@ -69,6 +69,8 @@ def lib():
             ("ref_ldu_cg", None, [P_] * 6 + [d, i, P_]),
             ("ref_green_gauss", None, [P_] * 3),
             ("ref_forces", i, [P_, d, d, d, d, d, P_, P_]),
+            ("ref_sweep_angles", i, [d, d, d, P_, i]),
+            ("ref_polar_csv", i, [C.c_char_p, C.c_char_p, d, d, d, d, i, i, P_, C.c_char_p, i]),
         ]:
             fn = getattr(_lib, name)
             fn.restype = res
@@ -221,3 +223,25 @@ class RefSolver:
         if lib().ref_forces(self._h, speed, alpha_deg, density, reynolds, chord, _p(out), _p(cp)) != 0:
             raise ValueError(lib().ref_last_error().decode())
         return out, cp[: int(out[5])]
+
+
+def sweep_angles(start, end, step):
+    """post::sweepAngles: the list of angles, or ValueError with the
+    reference's message."""
+    n = lib().ref_sweep_angles(start, end, step, None, 0)
+    if n < 0:
+        raise ValueError(lib().ref_last_error().decode())
+    out = np.zeros(max(n, 1))
+    lib().ref_sweep_angles(start, end, step, _p(out), n)
+    return out[:n].tolist()
+
+
+def polar_csv(section, mesh, reynolds, speed, chord, moment_reference, continued, points):
+    """post::toCsv of a polar; `points` is an (n, 13) array (see ref_polar_csv)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 13)
+    args = (section.encode(), mesh.encode(), reynolds, speed, chord, moment_reference,
+            1 if continued else 0, pts.shape[0], _p(pts))
+    n = lib().ref_polar_csv(*args, None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib().ref_polar_csv(*args, buf, n)
+    return buf.raw[:n].decode()

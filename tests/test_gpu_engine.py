@@ -125,3 +125,84 @@ def test_each_result_is_the_same_alone_and_in_the_mix_when_tuned():
         a, b = cb.Engine(chunk=16, tuned=True).run([req])[0], together[k]
         assert (a.status, a.iterations, a.cluster_size) == (b.status, b.iterations, b.cluster_size)
         assert a.lift_coefficient == pytest.approx(b.lift_coefficient, rel=1e-12, abs=1e-15)
+
+
+def _direct(mesh, alpha, cluster, start=None, tol=1e-8, cap=3000):
+    """A solve run by hand on the engine's launch shape (its bits depend on
+    the CTAs per solve), optionally from a given u, v, p."""
+    old = os.environ.get("CFD_CLUSTER_SIZE")
+    os.environ["CFD_CLUSTER_SIZE"] = str(cluster)
+    try:
+        s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha),
+                                   cb.Settings.defaults(inflow_viscosity_ratio=10.0))
+    finally:
+        if old is None:
+            os.environ.pop("CFD_CLUSTER_SIZE")
+        else:
+            os.environ["CFD_CLUSTER_SIZE"] = old
+    s.set_turbulence_model(cb.MODEL_SST)
+    u, v, p, rho, mu = cb.uniform_field(mesh, 1.0, alpha, 1.0, 1e6)
+    if start is not None:
+        u, v, p = start  # FlowField::uniform, then velocity and pressure carried over
+    s.initialise(u, v, p, rho, mu)
+    taken, _ = s.converge(cap, tol)
+    f, _, _ = s.forces(1.0, alpha, 1.0)
+    return s, taken, f
+
+
+def test_continued_sweep_is_the_reference_continuation():
+    """A continued polar sweep (startPolarSweep / updatePolar, Panels.cpp:1601-1797):
+    points in sweepAngles order, one after another, each after the first
+    started from the previous point's final u and p with density, viscosity,
+    k and omega from the freestream (Panels.cpp:1145-1156). The engine's
+    points equal the same chain run by hand, bit for bit."""
+    base = _req(alpha=0.0, tol=1e-8, cap=3000)
+    engine = cb.Engine(chunk=32)
+    ids = engine.submit_sweep(base, 0.0, 4.0, 2.0, continued=True)
+    res = sorted(engine.drain(), key=lambda r: r.id)
+    assert [r.id for r in res] == ids
+    assert [r.alpha_deg for r in res] == [0.0, 2.0, 4.0]
+    assert [r.continued for r in res] == [0, 1, 1]
+    assert all(r.status == 0 for r in res)
+    mesh = cb.cgrid("0012", upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0,
+                    **TINY)
+    start = None
+    for r in res:
+        s, taken, f = _direct(mesh, r.alpha_deg, r.cluster_size, start)
+        assert r.iterations == taken
+        assert r.lift_coefficient == pytest.approx(f.lift_coefficient, rel=1e-12, abs=1e-15)
+        assert r.drag_coefficient == pytest.approx(f.drag_coefficient, rel=1e-12)
+        start = (s.read("U"), s.read("V"), s.read("P"))
+        s.close()
+    # started cold, every point is the freestream solve; the same fixed point
+    cold = cb.Engine(chunk=32)
+    cold.submit_sweep(base, 0.0, 4.0, 2.0, continued=False)
+    rc = sorted(cold.drain(), key=lambda r: r.id)
+    assert [r.continued for r in rc] == [0, 0, 0]
+    assert rc[0].iterations == res[0].iterations
+    for a, b in zip(res, rc):
+        assert a.lift_coefficient == pytest.approx(b.lift_coefficient, abs=1e-5)
+
+
+def test_descending_sweep_and_many_sweeps_share_the_engine():
+    engine = cb.Engine(chunk=32)
+    down = engine.submit_sweep(_req(alpha=0.0, tol=1e-6), 4.0, 0.0, 2.0)
+    up = engine.submit_sweep(_req("2412", alpha=0.0, re=3e6, tol=1e-6), -2.0, 2.0, 2.0)
+    single = engine.submit(_req(alpha=1.0, tol=1e-6))
+    res = {r.id: r for r in engine.drain()}
+    assert sorted(res) == sorted(down + up + [single])
+    assert [res[i].alpha_deg for i in down] == [4.0, 2.0, 0.0]
+    assert [res[i].alpha_deg for i in up] == [-2.0, 0.0, 2.0]
+    assert res[single].continued == 0
+
+
+def test_a_request_that_cannot_start_is_reported_failed_not_diverged():
+    bad = _req(tol=1e-6)
+    bad.settings.velocity_relaxation = 1.5  # refused by SimpleSolver::create (SimpleSolver.cpp:41-44)
+    engine = cb.Engine(chunk=16)
+    one = engine.submit(bad)
+    sweep = engine.submit_sweep(bad, 0.0, 2.0, 1.0)
+    res = {r.id: r for r in engine.drain()}
+    for i in [one] + sweep:
+        assert res[i].status == 3 and res[i].error == 1, (i, res[i].status, res[i].error)
+    assert [res[i].alpha_deg for i in sweep] == [0.0, 1.0, 2.0]

@@ -55,6 +55,27 @@ def test_pipelined_sweeps_are_bit_identical_to_sequential_rows():
         assert np.array_equal(a[f], b[f]), f
 
 
+def test_shared_and_global_memory_cg_are_bit_identical():
+    # 384 x 96 on 16 CTAs: the pressure CG's band fits in shared memory by
+    # default and runs from global memory with flag bit 0; one algorithm,
+    # the same arithmetic and reduction order
+    a, ha = _medium_sst(6, 0)
+    b, hb = _medium_sst(6, 1)
+    assert np.array_equal(ha, hb)
+    for f in FIELDS:
+        assert np.array_equal(a[f], b[f]), f
+
+
+def test_single_reduction_cg_tracks_the_two_reduction_form():
+    # flag bit 3: the reference's two-reduction PCG; the single-reduction
+    # rearrangement computes the same iterates, up to rounding
+    a, ha = _medium_sst(1, 0)
+    b, hb = _medium_sst(1, 8)
+    assert np.max(np.abs(ha[:, 5] - hb[:, 5])) <= 1
+    for f in FIELDS:
+        assert rel_err(a[f], b[f]) < 1e-9, f
+
+
 @pytest.mark.parametrize("name", ["sst_cgrid", "sst_cambered"])
 @pytest.mark.parametrize("ctas", [6, 8])
 def test_wide_cluster_tracks_the_oracle(name, ctas):
