@@ -154,8 +154,9 @@ def _mesh(cb, designation, level, first_layer, cache):
     return cache[key]
 
 
-def polar_solvers(cb, precision: int = 0, cluster: int | None = None):
-    """The 24 solves of the batched polar, created on the device from the
+def polar_solvers(cb, precision: int = 0, cluster: int | None = None, count: int | None = None):
+    """The 24 solves of the batched polar (or its first `count`, for a
+    profiling capture of a smaller case), created on the device from the
     uniform start. `cluster` fixes the CTAs per solve (the library's
     CFD_CLUSTER_SIZE knob), else each solve takes the library's default."""
     settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
@@ -165,7 +166,7 @@ def polar_solvers(cb, precision: int = 0, cluster: int | None = None):
         os.environ["CFD_CLUSTER_SIZE"] = str(cluster)
     meshes, solvers = {}, []
     try:
-        for des, alpha, re, level, fl in POLAR:
+        for des, alpha, re, level, fl in POLAR[:count]:
             mesh = _mesh(cb, des, level, fl, meshes)
             s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
             s.set_turbulence_model(cb.MODEL_SST)
@@ -441,7 +442,8 @@ def run_ours(args) -> None:
     if c2:
         solvers = c2_solvers(cb, 1 if mixed_only else 0)
     else:
-        solvers = polar_solvers(cb, 1 if mixed_only else 0, MIXED_CLUSTER if mixed_only else None)
+        solvers = polar_solvers(cb, 1 if mixed_only else 0, MIXED_CLUSTER if mixed_only else None,
+                                args.solves)
     batch = cb.Batch(solvers)
     cells = sum(s.mesh.cells for s in solvers)
     # A stream of our own: events, the L2 flush and the solver launches all go
@@ -470,7 +472,7 @@ def run_ours(args) -> None:
         batch.close()
         for s in solvers:
             s.close()
-        m_solvers = polar_solvers(cb, 1, MIXED_CLUSTER)
+        m_solvers = polar_solvers(cb, 1, MIXED_CLUSTER, args.solves)
         m_batch = cb.Batch(m_solvers)
         m_ms, m_clocks = _timed_steps(torch, m_batch, handle, stream, flush, args.steps, args.warmup, dist)
         _, m_mon = m_batch.monitors()
@@ -493,7 +495,9 @@ def run_ours(args) -> None:
         profile = ("simple_kernel_c2_sst_mixed.md" if mixed_only else "simple_kernel_c2_sst_fp64.md") if c2 \
             else ("simple_kernel_polar_mixed.md" if mixed_only else "simple_kernel_polar_fp64.md")
         roofline = _roofline(solvers, cg, step_ms, mixed_only, profile)
-        config = c2_config() if c2 else polar_config()
+        config = c2_config() if c2 else polar_config({"solves": len(solvers), "cells": cells})
+        if not c2 and args.solves is not None:
+            config["workload"] += f" (only the first {len(solvers)} solves: a profiling case)"
         config.update({"cluster_shape": shape, "launch": "cuda graph" if args.graph else "direct",
                        "cg_iterations_per_solve": cg})
         if mixed_only:
@@ -562,6 +566,8 @@ def _summarise(results, wall_s, cb):
     return {"solves": len(results), "wall_s": wall_s, "solves_per_min": 60.0 * len(results) / wall_s,
             "cell_iters_per_s": cell_iters / wall_s, "statuses": statuses,
             "time_to_convergence_s": _percentiles(lat),
+            "queue_s": _percentiles([r.started_s - r.submitted_s for r in results]),
+            "mesh_s": _percentiles([r.mesh_s for r in results if r.mesh_s > 0.0]),
             "iterations": _percentiles([r.iterations for r in results])}
 
 
@@ -707,15 +713,16 @@ def serving_stream(n: int, rate: float, seed: int):
     return out
 
 
-def run_serve(args) -> None:
-    import torch
-    torch.cuda.set_device(0)
-    import cfd_b200 as cb
-    cb.set_device(0)
-    stream = serving_stream(args.requests, args.rate, args.seed)
-    settings = cb.Settings.defaults(inflow_viscosity_ratio=VISCOSITY_RATIO,
-                                    precision=1 if args.precision == "mixed" else 0)
-    engine = cb.Engine(chunk=args.chunk, tuned=True)  # a saturated GPU: the occupancy tuner
+def serve(cb, rate, requests, seed, precision, tolerance, cap, chunk) -> dict:
+    """One serving run: the seeded Poisson stream submitted to the engine in
+    real time (engine clock), stepped until every request has finished.
+    Time to convergence is finished - submitted per request, so it includes
+    queueing; the served rate says whether the GPU kept up with the offered
+    one (when it does not, the queue grows and the percentiles measure it)."""
+    stream = serving_stream(requests, rate, seed)
+    settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
+                                    precision=1 if precision == "mixed" else 0)
+    engine = cb.Engine(chunk=chunk, tuned=True)  # a saturated GPU: the occupancy tuner
     t0 = engine.clock()
     submitted, results = 0, []
     wall0 = time.perf_counter()
@@ -723,22 +730,41 @@ def run_serve(args) -> None:
         now = engine.clock() - t0
         while submitted < len(stream) and stream[submitted][0] <= now:
             _, des, alpha, re, level, fl = stream[submitted]
-            s, w, n = GRIDS[level]
-            engine.submit(cb.request(des, alpha, re, tolerance=args.tolerance,
-                                     max_iterations=args.cap, surface_points=s, wake_points=w,
-                                     normal_points=n, first_layer_height=fl, settings=settings))
+            sp, wp, npn = GRIDS[level]
+            engine.submit(cb.request(des, alpha, re, tolerance=tolerance, max_iterations=cap,
+                                     surface_points=sp, wake_points=wp, normal_points=npn,
+                                     first_layer_height=fl, settings=settings))
             submitted += 1
         active, queued = engine.step()
         results.extend(engine.results())
         if active == 0 and queued == 0 and submitted < len(stream):
             time.sleep(max(0.0, min(0.05, stream[submitted][0] - (engine.clock() - t0))))
     wall = time.perf_counter() - wall0
+    engine.close()
     out = _summarise(results, wall, cb)
-    out.update({"workload": f"serve: Poisson lambda={args.rate}/s, {args.requests} NACA 4-digit SST "
-                            f"requests (seed {args.seed}), meshes 192x48/384x96/768x192 at "
-                            "0.5/0.35/0.15", "precision": args.precision if args.precision == "mixed" else "plain",
-                "tolerance": args.tolerance, "cap": args.cap,
-                "chunk": args.chunk})
+    served = len(results) / wall
+    out.update({"workload": f"serve: Poisson lambda={rate:g}/s, {requests} NACA 4-digit SST "
+                            f"requests (seed {seed}), meshes 192x48/384x96/768x192 at "
+                            "0.5/0.35/0.15", "precision": precision,
+                "offered_per_s": rate, "served_per_s": served, "saturated": served < 0.9 * rate,
+                "tolerance": tolerance, "cap": cap, "chunk": chunk})
+    return out
+
+
+def run_serve(args) -> None:
+    """configs[4] at its own rate (lambda = 4/s), then, when the GPU could not
+    keep up with it, the same kind of stream at 70 % of the rate it served,
+    where the latency percentiles measure the solves rather than the queue."""
+    import torch
+    torch.cuda.set_device(0)
+    import cfd_b200 as cb
+    cb.set_device(0)
+    precision = "mixed" if args.precision == "mixed" else "plain"
+    out = serve(cb, args.rate, args.requests, args.seed, precision, args.tolerance, args.cap, args.chunk)
+    if out["saturated"]:
+        rate = 0.7 * out["served_per_s"]
+        out["sustainable"] = serve(cb, rate, max(64, args.requests // 4), args.seed + 1, precision,
+                                   args.tolerance, args.cap, args.chunk)
     print(json.dumps(out), flush=True)
 
 
@@ -756,6 +782,9 @@ def main() -> None:
     ap.add_argument("--workload", choices=("batch", "c2", "polar", "serve", "settled"), default="batch",
                     help="batch: the benchmark line, the 24-solve polar in one launch per step "
                          "(default); c2: the 384x96 pair; polar / serve / settled: engine workloads")
+    ap.add_argument("--solves", type=int, default=None,
+                    help="batch: time only the first N solves of the polar (a smaller case "
+                         "for profiling captures; the benchmark line uses all 24)")
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--cap", type=int, default=4000)
     ap.add_argument("--chunk", type=int, default=32)

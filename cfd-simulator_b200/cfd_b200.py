@@ -568,7 +568,7 @@ class Result(C.Structure):
                 ("started_s", C.c_double), ("finished_s", C.c_double),
                 ("separation_upper_chord_fraction", C.c_double),
                 ("separation_lower_chord_fraction", C.c_double), ("alpha_deg", C.c_double),
-                ("continued", C.c_int), ("error", C.c_int)]
+                ("continued", C.c_int), ("error", C.c_int), ("mesh_s", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

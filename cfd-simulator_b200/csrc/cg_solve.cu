@@ -5,10 +5,9 @@
 //
 // The iteration is the reference's, with its L1 stopping rule and its
 // breakdown guards; the dot products are summed in a fixed order (warp
-// trees, then CTA ranks in order), so a solve is deterministic. Two cluster
-// barriers per iteration: the next direction d' = z + beta d is formed for a
-// cell and, redundantly, for its neighbours from z and d, which are both
-// stable across the barrier.
+// trees, then CTA ranks in order), so a solve is deterministic. One cluster
+// barrier per iteration: the single-reduction arrangement described at
+// cgSolveTeam.
 
 #include <cuda_runtime.h>
 
@@ -33,7 +32,7 @@ struct CgView {
   const double* pN;
   const double* pE;
   const double* b;
-  double *x, *r, *z, *q, *d0, *d1;
+  double *x, *r, *z, *q, *d0, *d1, *s1, *p;
   int maxIt;
   double tol;
   double* report;  // {iterations, initial, final, converged, bad wake map}: 8 words
@@ -55,78 +54,110 @@ DEV double precondition(double rc, double dg) { return (fabs(dg) > 0.0) ? rc / d
 
 }  // namespace
 
-/// The whole solve, run by every thread of the cluster.
+/// y = A v at cell c for a v given as a function of the cell (the matrix
+/// row in multiply's face order).
+template <typename F>
+DEV double rowApply(const CgView& V, int c, int i, int j, double vc, F&& v) {
+  double y = V.diag[c] * vc;
+  if (j > 0) y += V.pN[j * V.NI + i] * v(c - V.NI);
+  else if (V.acrossJ0[i] >= 0) y += V.pN[i] * v(V.acrossJ0[i]);
+  if (j < V.NJ - 1) y += V.pN[(j + 1) * V.NI + i] * v(c + V.NI);
+  if (i > 0) y += V.pE[j * (V.NI + 1) + i] * v(c - 1);
+  if (i < V.NI - 1) y += V.pE[j * (V.NI + 1) + i + 1] * v(c + 1);
+  return y;
+}
+
+/// The whole solve, run by every thread of the cluster: the reference's
+/// Jacobi-PCG rearranged with one reduction per iteration (Chronopoulos and
+/// Gear, 1989), as in the SIMPLE kernel's pressure solve: u = M^-1 r,
+/// w = A u, one reduction of {r.u, w.u, sum |r|}; beta = gamma'/gamma,
+/// d.Ad = delta' - beta gamma'/alpha, alpha = gamma'/d.Ad; p = u + beta p,
+/// s = w + beta s, x += alpha p, r -= alpha s. The reference's L1 stopping
+/// rule, cap and breakdown guards; the same iterates to rounding. r, w and s
+/// are double-buffered ((r, z), (q, d0), (d1, s1)) so a cell can form its
+/// neighbours' next u from their values of this iteration.
 __device__ void cgSolveTeam(const CgView& V, Team& t, Shared& sh) {
-  const int op2[2] = {kSum, kSum};
+  double* rB[2] = {V.r, V.z};
+  double* wB[2] = {V.q, V.d0};
+  double* sB[2] = {V.d1, V.s1};
   const int op1[1] = {kSum};
+  const int op2[2] = {kSum, kSum};
+  const int op3[3] = {kSum, kSum, kSum};
   double init[2] = {0.0, 0.0};
   for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
     const int i = c % V.NI, j = c / V.NI;
     const double rc = V.b[c] - rowTimes(V, c, i, j, V.x, V.x[c]);
-    const double zc = precondition(rc, V.diag[c]);
-    V.r[c] = rc;
-    V.z[c] = zc;
-    V.d0[c] = zc;
+    rB[0][c] = rc;
+    sB[0][c] = 0.0;
+    V.p[c] = 0.0;
     init[0] += fabs(rc);
-    init[1] += rc * zc;
+    init[1] += rc * precondition(rc, V.diag[c]);
   }
   teamReduce(t, sh, init, op2);
   const double initial = init[0];
-  double rz = init[1];
   double finalResidual = initial;
   int iterations = 0;
   bool converged = false;
   if (initial <= 0.0) {
     converged = true;
   } else {
-    double* dCur = V.d0;
-    double* dNext = V.d1;
-    double beta = 0.0;
-    for (int iter = 0; iter < V.maxIt; ++iter) {
-      double dAd[1] = {0.0};
-      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        const int i = c % V.NI, j = c / V.NI;
-        double dc;
-        if (iter == 0) {
-          dc = dCur[c];
-          V.q[c] = rowTimes(V, c, i, j, dCur, dc);
-        } else {
-          dc = V.z[c] + beta * dCur[c];
-          dNext[c] = dc;
-          double y = V.diag[c] * dc;
-          int n = (j > 0) ? c - V.NI : V.acrossJ0[i];
-          if (n >= 0) y += V.pN[j * V.NI + i] * (V.z[n] + beta * dCur[n]);
-          if (j < V.NJ - 1) { n = c + V.NI; y += V.pN[(j + 1) * V.NI + i] * (V.z[n] + beta * dCur[n]); }
-          if (i > 0) { n = c - 1; y += V.pE[j * (V.NI + 1) + i] * (V.z[n] + beta * dCur[n]); }
-          if (i < V.NI - 1) { n = c + 1; y += V.pE[j * (V.NI + 1) + i + 1] * (V.z[n] + beta * dCur[n]); }
-          V.q[c] = y;
+    // w0 = A u0: every r0 is in place since the reduction's barrier
+    double acc[1] = {0.0};
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % V.NI, j = c / V.NI;
+      const double un = precondition(rB[0][c], V.diag[c]);
+      const double y = rowApply(V, c, i, j, un, [&](int n) { return precondition(rB[0][n], V.diag[n]); });
+      wB[0][c] = y;
+      acc[0] += y * un;
+    }
+    teamReduce(t, sh, acc, op1);
+    if (fabs(acc[0]) > 0.0) {
+      double gamma = init[1], alpha = gamma / acc[0], beta = 0.0;
+      int cur = 0;
+      for (int iter = 0; iter < V.maxIt; ++iter) {
+        const double* r = rB[cur];
+        const double* w = wB[cur];
+        const double* sv = sB[cur];
+        double* rn = rB[cur ^ 1];
+        double* wn = wB[cur ^ 1];
+        double* sn = sB[cur ^ 1];
+        double sums[3] = {0.0, 0.0, 0.0};
+        for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+          const int i = c % V.NI, j = c / V.NI;
+          const double dg = V.diag[c];
+          const double pc = precondition(r[c], dg) + beta * V.p[c];
+          const double sc = w[c] + beta * sv[c];
+          V.x[c] += alpha * pc;
+          const double rc = r[c] - alpha * sc;
+          const double un = precondition(rc, dg);
+          const double y = rowApply(V, c, i, j, un, [&](int n) {
+            const double s2 = w[n] + beta * sv[n];
+            return precondition(r[n] - alpha * s2, V.diag[n]);
+          });
+          V.p[c] = pc;
+          sn[c] = sc;
+          rn[c] = rc;
+          wn[c] = y;
+          sums[0] += rc * un;
+          sums[1] += y * un;
+          sums[2] += fabs(rc);
         }
-        dAd[0] += dc * V.q[c];
+        cur ^= 1;
+        teamReduce(t, sh, sums, op3);
+        iterations = iter + 1;
+        finalResidual = sums[2];
+        if (sums[2] <= V.tol * initial) {
+          converged = true;
+          break;
+        }
+        if (!(fabs(gamma) > 0.0)) break;
+        const double nextBeta = sums[0] / gamma;
+        const double dAd = sums[1] - nextBeta * sums[0] / alpha;
+        if (!(fabs(dAd) > 0.0)) break;
+        beta = nextBeta;
+        alpha = sums[0] / dAd;
+        gamma = sums[0];
       }
-      if (iter > 0) { double* tmp = dCur; dCur = dNext; dNext = tmp; }
-      teamReduce(t, sh, dAd, op1);
-      if (!(fabs(dAd[0]) > 0.0)) break;
-      const double step = rz / dAd[0];
-      double rr[2] = {0.0, 0.0};
-      for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-        V.x[c] += step * dCur[c];
-        const double rc = V.r[c] - step * V.q[c];
-        V.r[c] = rc;
-        const double zc = precondition(rc, V.diag[c]);
-        V.z[c] = zc;
-        rr[0] += fabs(rc);
-        rr[1] += rc * zc;
-      }
-      teamReduce(t, sh, rr, op2);
-      iterations = iter + 1;
-      finalResidual = rr[0];
-      if (rr[0] <= V.tol * initial) {
-        converged = true;
-        break;
-      }
-      if (!(fabs(rz) > 0.0)) break;
-      beta = rr[1] / rz;
-      rz = rr[1];
     }
   }
   if (t.rank == 0 && t.tid == 0 && V.report != nullptr) {
@@ -256,9 +287,9 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   const std::size_t N = V.N;
   const std::size_t FN = static_cast<std::size_t>(V.NI) * (V.NJ + 1);
   const std::size_t FE = static_cast<std::size_t>(V.NI + 1) * V.NJ;
-  // Scratch for this call: both coefficient families, five CG vectors, the
+  // Scratch for this call: both coefficient families, seven CG vectors, the
   // report (8 words) and the wake map.
-  const std::size_t doubles = FN + FE + 5 * N + 8;
+  const std::size_t doubles = FN + FE + 7 * N + 8;
   char* scratch = nullptr;
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&scratch), doubles * sizeof(double) + V.NI * sizeof(int));
   if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
@@ -270,6 +301,8 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
   V.q = p; p += N;
   V.d0 = p; p += N;
   V.d1 = p; p += N;
+  V.s1 = p; p += N;
+  V.p = p; p += N;
   V.report = p; p += 8;
   V.acrossJ0 = reinterpret_cast<const int*>(p);
   V.diag = system->diag;
@@ -293,22 +326,24 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
 // fails or breaks its accounting), or a latency-critical loop that must not
 // block on the implicit device-wide synchronisation cudaFree performs.
 // cfd_cg_solve_noalloc serves them. Its scratch (both coefficient families,
-// the five CG vectors, the wake map and the report) is one file-scope device
+// the seven CG vectors, the wake map and the report) is one file-scope device
 // array of fixed size, so a call allocates nothing; the caller still provides
 // the system and x in its own device memory.
 //
 // Limits and sharing:
 //   * blocks of at most kNoAllocMaxNodes mesh nodes, (cells_i+1)*(cells_j+1)
 //     <= 65,536 (the 384 x 96 medium C-grid has 37,345); larger blocks are
-//     refused with CFD_OUT_OF_RANGE. The array is 3.8 MiB, held by every GPU
+//     refused with CFD_OUT_OF_RANGE. The array is 4.75 MiB, held by every GPU
 //     that loads this library until the process exits.
 //   * every call shares the one array per device and it keeps the last
-//     call's contents. Nothing in it needs clearing: each word a solve reads is
-//     written earlier in the same call (coefficients and wake map by the layout
-//     launch, r, z and d0 from the start vector, q and d1 before their first
-//     use). Calls whose work overlaps on the GPU (other host threads, or other
-//     streams of this one) race on the array and must be serialised by the
-//     caller.
+//     call's contents. Nothing in it needs clearing beforehand: each word a
+//     solve reads is written earlier in the same call (coefficients and wake
+//     map by the layout launch; the first residual, w and the zero p and s
+//     at the start of the solve; each later half of the double-buffered r, w
+//     and s in the iteration before it is read), and the error flag is
+//     cleared by the call itself. Calls whose work overlaps on the GPU (other
+//     host threads, or other streams of this one) race on the array and must
+//     be serialised by the caller.
 //   * the first call on each device resolves the array's device address with
 //     cudaGetSymbolAddress, with that device current; make that first call
 //     before any stream capture begins. Every call waits for its solve to
@@ -320,11 +355,11 @@ namespace cfdb {
 namespace {
 
 constexpr long long kNoAllocMaxNodes = 65536;
-// 7 arrays of at most kNoAllocMaxNodes doubles (two face families and five
+// 9 arrays of at most kNoAllocMaxNodes doubles (two face families and seven
 // cell vectors, each at most (cells_i+1)*(cells_j+1) long), 8 report words,
 // and the wake map (cells_i <= 32,767 ints) in the last kNoAllocMaxNodes/2
-// doubles.
-constexpr std::size_t kNoAllocDoubles = 7 * kNoAllocMaxNodes + 8 + kNoAllocMaxNodes / 2;
+// doubles: 4.75 MiB.
+constexpr std::size_t kNoAllocDoubles = 9 * kNoAllocMaxNodes + 8 + kNoAllocMaxNodes / 2;
 
 static __device__ __align__(256) double g_noAllocScratch[kNoAllocDoubles];
 
@@ -377,8 +412,10 @@ cfd_status cfd_cg_solve_noalloc(const cfd_cg_system* system, double* x, double t
   V.q = base + 4 * slot;
   V.d0 = base + 5 * slot;
   V.d1 = base + 6 * slot;
-  V.report = base + 7 * slot;
-  V.acrossJ0 = reinterpret_cast<const int*>(base + 7 * slot + 8);
+  V.s1 = base + 7 * slot;
+  V.p = base + 8 * slot;
+  V.report = base + 9 * slot;
+  V.acrossJ0 = reinterpret_cast<const int*>(base + 9 * slot + 8);
   V.diag = system->diag;
   V.b = system->source;
   V.x = x;

@@ -22,11 +22,15 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <deque>
+#include <functional>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -45,6 +49,86 @@ namespace {
 constexpr double kPi = 3.14159265358979323846;  // the double std::numbers::pi rounds to
 constexpr int kMaxSweepPoints = 400;               // post::kMaxSweepPoints (Polar.hpp)
 
+/// A C-grid built for a request: the mesh, or the generator's refusal.
+struct MeshResult {
+  std::shared_ptr<const HostMesh> mesh;
+  Status status{CFD_OK};
+  std::string message;
+  double seconds{0.0};  // generation time
+};
+using MeshFuture = std::shared_future<MeshResult>;
+
+/// Host C-grid generation off the caller's thread. generateCGrid +
+/// buildStructured (src/mesh/CGrid.cpp:98-399, src/mesh/Mesh.cpp:89-339) take
+/// tens of milliseconds for a fine grid; a serving stream draws a new section,
+/// Reynolds number and first-layer height per request, so most requests need
+/// a grid of their own. Workers build them while the GPU runs, and a request
+/// is admitted once its mesh is ready.
+class MeshPool {
+ public:
+  explicit MeshPool(int threads) {
+    for (int k = 0; k < threads; ++k) workers_.emplace_back([this] { run(); });
+  }
+  MeshPool(const MeshPool&) = delete;
+  MeshPool& operator=(const MeshPool&) = delete;
+  ~MeshPool() {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      stop_ = true;
+    }
+    wake_.notify_all();
+    for (std::thread& t : workers_) t.join();
+  }
+
+  MeshFuture build(std::string designation, const cfd_cgrid_options& o) {
+    std::packaged_task<MeshResult()> task([designation = std::move(designation), o] {
+      MeshResult r;
+      const auto t0 = std::chrono::steady_clock::now();
+      auto m = std::make_shared<HostMesh>();
+      r.status = makeCGrid(designation.c_str(), o, m.get());
+      if (r.status == CFD_OK) {
+        r.mesh = std::move(m);
+      } else {
+        r.message = cfd_last_error();  // the worker's own message
+      }
+      r.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      return r;
+    });
+    MeshFuture f = task.get_future().share();
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      tasks_.push_back(std::move(task));
+    }
+    wake_.notify_one();
+    return f;
+  }
+
+ private:
+  void run() {
+    for (;;) {
+      std::packaged_task<MeshResult()> task;
+      {
+        std::unique_lock<std::mutex> lock(mutex_);
+        wake_.wait(lock, [this] { return stop_ || !tasks_.empty(); });
+        if (tasks_.empty()) return;  // stopping, nothing left
+        task = std::move(tasks_.front());
+        tasks_.pop_front();
+      }
+      task();
+    }
+  }
+
+  std::vector<std::thread> workers_;
+  std::deque<std::packaged_task<MeshResult()>> tasks_;
+  std::mutex mutex_;
+  std::condition_variable wake_;
+  bool stop_{false};
+};
+
+bool ready(const MeshFuture& f) {
+  return f.wait_for(std::chrono::seconds(0)) == std::future_status::ready;
+}
+
 /// A start other than the freestream: the u, v and p a continued polar point
 /// takes over from the previous point (src/app/Panels.cpp:1145-1156).
 struct WarmStart {
@@ -61,6 +145,7 @@ struct Slot {
   bool continued{false};
   int sweep{-1};  // index of the sweep this point belongs to, or -1
   int point{0};   // its position in that sweep
+  double meshSeconds{0.0};
   double submitted{0.0}, started{0.0};
   std::size_t bytes{0};
 };
@@ -68,7 +153,10 @@ struct Slot {
 struct Pending {
   int id{0};
   cfd_request request{};
-  std::shared_ptr<const HostMesh> mesh;
+  std::shared_ptr<const HostMesh> mesh;  // set once the mesh is ready
+  MeshFuture meshFuture;                 // the mesh being built, when not yet known
+  bool builtMesh{false};                 // this request's submit started the build
+  double meshSeconds{0.0};
   double submitted{0.0};
   int sweep{-1};
   int point{0};
@@ -114,8 +202,13 @@ struct Engine {
   std::vector<std::unique_ptr<Slot>> active;
   std::vector<cfd_result> done;
   std::map<int, std::vector<double>> surfaces;  // Cp per wall station of each finished solve
-  std::map<MeshKey, std::shared_ptr<const HostMesh>> meshes;
+  std::map<MeshKey, MeshFuture> meshes;  // every grid requested so far, built or being built
+  std::unique_ptr<MeshPool> pool;
   std::chrono::steady_clock::time_point t0{std::chrono::steady_clock::now()};
+  // the chunk in flight: its launches run while step() returns to the caller
+  bool inFlight{false};
+  int inFlightSlots{0};
+  std::vector<int> inFlightStreams;
   // device status area: per slot, chunk monitors then the iteration count
   double* dStatus{nullptr};
   int statusSlots{0};
@@ -128,6 +221,7 @@ struct Engine {
   }
 
   ~Engine() {
+    waitForLaunches();
     active.clear();
     if (dStatus) cudaFree(dStatus);
     if (dTable) cudaFree(dTable);
@@ -185,6 +279,7 @@ struct Engine {
     slot->continued = (q.warm != nullptr);
     slot->sweep = q.sweep;
     slot->point = q.point;
+    slot->meshSeconds = q.meshSeconds;
     slot->submitted = q.submitted;
     slot->started = now();
     *out = std::move(slot);
@@ -378,23 +473,39 @@ struct Engine {
     }
   }
 
-  Status admit() {
-    while (!queue.empty()) {
-      const Pending& q = queue.front();
+  /// Start queued requests whose mesh is ready, in queue order, while they
+  /// fit the memory budget, appending them to `into`; a request whose mesh is
+  /// still being built keeps its place. An engine with nothing resident always
+  /// takes one, so an oversized request cannot stall the queue.
+  void admit(std::vector<std::unique_ptr<Slot>>& into, std::size_t resident) {
+    for (auto it = queue.begin(); it != queue.end();) {
+      Pending& q = *it;
+      if (!q.mesh) {
+        if (!ready(q.meshFuture)) {
+          ++it;
+          continue;
+        }
+        const MeshResult& m = q.meshFuture.get();
+        if (m.status != CFD_OK) {
+          failStart(q, m.status);
+          it = queue.erase(it);
+          continue;
+        }
+        q.mesh = m.mesh;
+        if (q.builtMesh) q.meshSeconds = m.seconds;
+      }
       const std::size_t need = Solver::estimateBytes(q.mesh->nodesI - 1, q.mesh->nodesJ - 1);
-      // always admit into an empty engine, so one oversized request cannot stall the queue
-      if (!active.empty() && used + need > budget) break;
+      if (resident + into.size() > 0 && used + need > budget) break;
       std::unique_ptr<Slot> slot;
       if (Status st = start(q, &slot); st != CFD_OK) {
         failStart(q, st);
-        queue.pop_front();
+        it = queue.erase(it);
         continue;
       }
       used += slot->bytes;
-      active.push_back(std::move(slot));
-      queue.pop_front();
+      into.push_back(std::move(slot));
+      it = queue.erase(it);
     }
-    return ok();
   }
 
   void finish(Slot& s, int status, const double* mon) {
@@ -405,6 +516,7 @@ struct Engine {
     r.retried_cold = s.retried ? 1 : 0;
     r.continued = s.continued ? 1 : 0;
     r.alpha_deg = s.request.alpha_deg;
+    r.mesh_s = s.meshSeconds;
     r.cells = s.solver->cells();
     r.cluster_size = s.solver->clusterSize();
     r.continuity = mon[kMonContinuity];
@@ -434,100 +546,145 @@ struct Engine {
     done.push_back(r);
   }
 
-  Status step(int* activeOut, int* queuedOut) {
-    if (Status st = admit(); st != CFD_OK) return st;
+  /// Launch `chunk` iterations of every resident solve, one launch per
+  /// launch shape over a descriptor table, and return without waiting.
+  Status launchChunk() {
     const int n = static_cast<int>(active.size());
-    if (n > 0) {
-      if (Status st = reserve(n); st != CFD_OK) return st;
-      // group by launch shape; table rows in slot order within each group
-      std::map<std::pair<int, int>, std::vector<int>> groups;
-      for (int k = 0; k < n; ++k) {
-        const Solver& s = *active[k]->solver;
-        groups[{s.clusterSize(), s.threads()}].push_back(k);
-      }
-      std::vector<Instance> table(n);
-      std::vector<std::tuple<int, int, int, int, int>> launches;  // offset, count, R, T, smem
-      const std::size_t per = static_cast<std::size_t>(chunk) * kMonSlots + 1;
-      int offset = 0;
-      for (const auto& [shape, members] : groups) {
-        int smem = 0;
-        for (std::size_t m = 0; m < members.size(); ++m) {
-          const int k = members[m];
-          Slot& s = *active[k];
-          Instance I = s.solver->deviceView();
-          double* status = dStatus + static_cast<std::size_t>(k) * per;
-          I.history = status;
-          I.iterations = reinterpret_cast<int*>(status + static_cast<std::size_t>(chunk) * kMonSlots);
-          I.stopTol = s.request.tolerance;
-          I.iterLimit = std::max(1, std::min(chunk, s.request.max_iterations - s.iterations));
-          table[offset + static_cast<int>(m)] = I;
-          smem = std::max(smem, s.solver->launchSmemBytes(shape.first));
-        }
-        launches.emplace_back(offset, static_cast<int>(members.size()), shape.first, shape.second, smem);
-        offset += static_cast<int>(members.size());
-      }
-      if (cudaMemcpy(dTable, table.data(), n * sizeof(Instance), cudaMemcpyHostToDevice) != cudaSuccess) {
-        return fail(CFD_INITIALIZATION_FAILURE, "engine table upload failed");
-      }
-      while (streams.size() < launches.size()) {
-        cudaStream_t s;
-        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
-          return fail(CFD_INITIALIZATION_FAILURE, "engine stream creation failed");
-        }
-        streams.push_back(s);
-      }
-      for (std::size_t g = 0; g < launches.size(); ++g) {
-        const auto [off, count, R, T, smem] = launches[g];
-        if (Status st = launchSimple(dTable + off, count, R, T, chunk, kStageEnd, -1.0, streams[g], smem);
-            st != CFD_OK) {
-          return st;
-        }
-      }
-      if (cudaDeviceSynchronize() != cudaSuccess) {
-        return fail(CFD_INITIALIZATION_FAILURE, "engine step failed on the device");
-      }
-      std::vector<double> status(static_cast<std::size_t>(n) * per);
-      if (cudaMemcpy(status.data(), dStatus, status.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
-          cudaSuccess) {
-        return fail(CFD_INITIALIZATION_FAILURE, "engine status read failed");
-      }
-      std::vector<std::unique_ptr<Slot>> keep;
-      for (int k = 0; k < n; ++k) {
+    if (Status st = reserve(n); st != CFD_OK) return st;
+    // group by launch shape; table rows in slot order within each group
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    for (int k = 0; k < n; ++k) {
+      const Solver& s = *active[k]->solver;
+      groups[{s.clusterSize(), s.threads()}].push_back(k);
+    }
+    std::vector<Instance> table(n);
+    std::vector<std::tuple<int, int, int, int, int>> launches;  // offset, count, R, T, smem
+    const std::size_t per = static_cast<std::size_t>(chunk) * kMonSlots + 1;
+    int offset = 0;
+    for (const auto& [shape, members] : groups) {
+      int smem = 0;
+      for (std::size_t m = 0; m < members.size(); ++m) {
+        const int k = members[m];
         Slot& s = *active[k];
-        const double* st = status.data() + static_cast<std::size_t>(k) * per;
-        int ran = 0;
-        std::memcpy(&ran, st + static_cast<std::size_t>(chunk) * kMonSlots, sizeof(int));
-        s.iterations += ran;
-        const double* mon = st + static_cast<std::size_t>(std::max(ran, 1) - 1) * kMonSlots;
-        const double a = mon[kMonContinuity], b = mon[kMonMomX], c = mon[kMonMomY];
-        const bool finite = std::isfinite(a) && std::isfinite(b) && std::isfinite(c);
-        int outcome = -1;
-        if (!finite) {
-          if (!s.retried) {
-            // RetryCold: restart once from the freestream
-            s.retried = true;
-            std::vector<double> u, v, p, rho, mu;
-            uniform(s.request, s.solver->cells(), &u, &v, &p, &rho, &mu);
-            if (s.solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()) != CFD_OK) {
-              outcome = CFD_SOLVE_DIVERGED;
-            }
-          } else {
+        Instance I = s.solver->deviceView();
+        double* status = dStatus + static_cast<std::size_t>(k) * per;
+        I.history = status;
+        I.iterations = reinterpret_cast<int*>(status + static_cast<std::size_t>(chunk) * kMonSlots);
+        I.stopTol = s.request.tolerance;
+        I.iterLimit = std::max(1, std::min(chunk, s.request.max_iterations - s.iterations));
+        table[offset + static_cast<int>(m)] = I;
+        smem = std::max(smem, s.solver->launchSmemBytes(shape.first));
+      }
+      launches.emplace_back(offset, static_cast<int>(members.size()), shape.first, shape.second, smem);
+      offset += static_cast<int>(members.size());
+    }
+    if (cudaMemcpy(dTable, table.data(), n * sizeof(Instance), cudaMemcpyHostToDevice) != cudaSuccess) {
+      return fail(CFD_INITIALIZATION_FAILURE, "engine table upload failed");
+    }
+    while (streams.size() < launches.size()) {
+      cudaStream_t s;
+      if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        return fail(CFD_INITIALIZATION_FAILURE, "engine stream creation failed");
+      }
+      streams.push_back(s);
+    }
+    inFlightStreams.clear();
+    for (std::size_t g = 0; g < launches.size(); ++g) {
+      const auto [off, count, R, T, smem] = launches[g];
+      if (Status st = launchSimple(dTable + off, count, R, T, chunk, kStageEnd, -1.0, streams[g], smem);
+          st != CFD_OK) {
+        waitForLaunches();
+        return st;
+      }
+      inFlightStreams.push_back(static_cast<int>(g));
+    }
+    inFlight = true;
+    inFlightSlots = n;
+    return ok();
+  }
+
+  /// Wait for the chunk in flight (its streams only, so the admission work
+  /// queued meanwhile on the new solves' own streams is not waited for).
+  Status waitForLaunches() {
+    Status st = ok();
+    for (int g : inFlightStreams) {
+      if (cudaStreamSynchronize(streams[static_cast<std::size_t>(g)]) != cudaSuccess && st == CFD_OK) {
+        st = fail(CFD_INITIALIZATION_FAILURE, "engine step failed on the device");
+      }
+    }
+    inFlightStreams.clear();
+    inFlight = false;
+    return st;
+  }
+
+  /// Read every launched solve's monitors and iteration count, and retire
+  /// the ones that converged, diverged (after one cold retry) or hit their cap.
+  Status retire() {
+    const int n = inFlightSlots;
+    const std::size_t per = static_cast<std::size_t>(chunk) * kMonSlots + 1;
+    std::vector<double> status(static_cast<std::size_t>(n) * per);
+    if (cudaMemcpy(status.data(), dStatus, status.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
+        cudaSuccess) {
+      return fail(CFD_INITIALIZATION_FAILURE, "engine status read failed");
+    }
+    std::vector<std::unique_ptr<Slot>> keep;
+    for (int k = 0; k < n; ++k) {
+      Slot& s = *active[k];
+      const double* st = status.data() + static_cast<std::size_t>(k) * per;
+      int ran = 0;
+      std::memcpy(&ran, st + static_cast<std::size_t>(chunk) * kMonSlots, sizeof(int));
+      s.iterations += ran;
+      const double* mon = st + static_cast<std::size_t>(std::max(ran, 1) - 1) * kMonSlots;
+      const double a = mon[kMonContinuity], b = mon[kMonMomX], c = mon[kMonMomY];
+      const bool finite = std::isfinite(a) && std::isfinite(b) && std::isfinite(c);
+      int outcome = -1;
+      if (!finite) {
+        if (!s.retried) {
+          // RetryCold: restart once from the freestream
+          s.retried = true;
+          std::vector<double> u, v, p, rho, mu;
+          uniform(s.request, s.solver->cells(), &u, &v, &p, &rho, &mu);
+          if (s.solver->initialise(u.data(), v.data(), p.data(), rho.data(), mu.data()) != CFD_OK) {
             outcome = CFD_SOLVE_DIVERGED;
           }
-        } else if (std::max({std::abs(a), std::abs(b), std::abs(c)}) < s.request.tolerance) {
-          outcome = CFD_SOLVE_CONVERGED;
-        } else if (s.iterations >= s.request.max_iterations) {
-          outcome = CFD_SOLVE_ITERATION_LIMIT;
-        }
-        if (outcome >= 0) {
-          finish(s, outcome, mon);
-          if (s.sweep >= 0) advanceSweep(s, outcome);
-          used -= s.bytes;
         } else {
-          keep.push_back(std::move(active[k]));
+          outcome = CFD_SOLVE_DIVERGED;
         }
+      } else if (std::max({std::abs(a), std::abs(b), std::abs(c)}) < s.request.tolerance) {
+        outcome = CFD_SOLVE_CONVERGED;
+      } else if (s.iterations >= s.request.max_iterations) {
+        outcome = CFD_SOLVE_ITERATION_LIMIT;
       }
-      active = std::move(keep);
+      if (outcome >= 0) {
+        finish(s, outcome, mon);
+        if (s.sweep >= 0) advanceSweep(s, outcome);
+        used -= s.bytes;
+      } else {
+        keep.push_back(std::move(active[k]));
+      }
+    }
+    for (std::size_t k = static_cast<std::size_t>(n); k < active.size(); ++k) keep.push_back(std::move(active[k]));
+    active = std::move(keep);
+    return ok();
+  }
+
+  /// One engine step. While the chunk launched by the previous step runs,
+  /// the requests that can join the next one are set up on the host (their
+  /// solvers built, initialised and copied to the device on their own
+  /// streams); then the step waits for the chunk, retires what finished,
+  /// fills the memory that freed, launches the next chunk and returns with it
+  /// running, so the caller's own work overlaps the GPU too.
+  Status step(int* activeOut, int* queuedOut) {
+    if (inFlight) {
+      std::vector<std::unique_ptr<Slot>> staged;
+      admit(staged, active.size());
+      if (Status st = waitForLaunches(); st != CFD_OK) return st;
+      if (Status st = retire(); st != CFD_OK) return st;
+      for (auto& slot : staged) active.push_back(std::move(slot));
+    }
+    admit(active, active.size());
+    if (!active.empty()) {
+      if (Status st = launchChunk(); st != CFD_OK) return st;
     }
     if (activeOut) *activeOut = static_cast<int>(active.size());
     if (queuedOut) *queuedOut = static_cast<int>(queue.size());
@@ -570,14 +727,19 @@ cfd_status checkRequest(const cfd_request* r) {
   return CFD_OK;
 }
 
-/// The request's C-grid, generated on first use and cached per grid.
-cfd_status meshFor(cfdb::Engine& g, const cfd_request& r, std::shared_ptr<const cfdb::HostMesh>* out) {
+/// The request's C-grid: from the engine's cache (built, or still being
+/// built), else queued on the engine's mesh workers. *built tells whether
+/// this call started the build.
+cfdb::MeshFuture meshFor(cfdb::Engine& g, const cfd_request& r, bool* built) {
   const cfdb::MeshKey key = cfdb::keyOf(r);
   if (auto it = g.meshes.find(key); it != g.meshes.end()) {
-    *out = it->second;
-    return CFD_OK;
+    *built = false;
+    return it->second;
   }
-  auto m = std::make_shared<cfdb::HostMesh>();
+  if (!g.pool) {
+    const unsigned cores = std::max(2u, std::thread::hardware_concurrency());
+    g.pool = std::make_unique<cfdb::MeshPool>(static_cast<int>(std::min(8u, cores / 2)));
+  }
   cfd_cgrid_options o;
   cfd_default_cgrid_options(&o);
   o.surface_points = r.grid_surface_points;
@@ -587,12 +749,11 @@ cfd_status meshFor(cfdb::Engine& g, const cfd_request& r, std::shared_ptr<const 
   o.upstream_chords = r.grid_upstream_chords;
   o.downstream_chords = r.grid_downstream_chords;
   o.vertical_chords = r.grid_vertical_chords;
-  char name[9] = {0};
-  std::memcpy(name, r.designation, 8);
-  if (cfd_status st = cfdb::makeCGrid(name, o, m.get()); st != CFD_OK) return st;
-  g.meshes[key] = m;
-  *out = m;
-  return CFD_OK;
+  const std::string name(r.designation, strnlen(r.designation, sizeof(r.designation)));
+  cfdb::MeshFuture f = g.pool->build(name, o);
+  g.meshes[key] = f;
+  *built = true;
+  return f;
 }
 
 }  // namespace
@@ -601,12 +762,10 @@ cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* r, int* id) {
   if (e == nullptr || r == nullptr) return cfdb::fail(CFD_INVALID_ARGUMENT, "null argument");
   if (cfd_status st = checkRequest(r); st != CFD_OK) return st;
   cfdb::Engine& g = e->engine;
-  std::shared_ptr<const cfdb::HostMesh> mesh;
-  if (cfd_status st = meshFor(g, *r, &mesh); st != CFD_OK) return st;
   cfdb::Pending q;
   q.id = g.nextId++;
   q.request = *r;
-  q.mesh = mesh;
+  q.meshFuture = meshFor(g, *r, &q.builtMesh);
   q.submitted = g.now();
   g.queue.push_back(q);
   if (id != nullptr) *id = q.id;
@@ -654,8 +813,6 @@ cfd_status cfd_engine_submit_sweep(cfd_engine e, const cfd_request* base, double
   sw.base = *base;
   sw.angles.resize(static_cast<std::size_t>(n));
   if (cfd_status st = cfd_sweep_angles(start, end, step, sw.angles.data(), n, &n); st != CFD_OK) return st;
-  std::shared_ptr<const cfdb::HostMesh> mesh;
-  if (cfd_status st = meshFor(g, *base, &mesh); st != CFD_OK) return st;
   sw.firstId = g.nextId;
   sw.continued = (continued != 0);
   g.nextId += n;
@@ -663,7 +820,7 @@ cfd_status cfd_engine_submit_sweep(cfd_engine e, const cfd_request* base, double
   q.id = sw.firstId;
   q.request = *base;
   q.request.alpha_deg = sw.angles.front();
-  q.mesh = mesh;
+  q.meshFuture = meshFor(g, *base, &q.builtMesh);
   q.submitted = g.now();
   q.sweep = static_cast<int>(g.sweeps.size());
   q.point = 0;

@@ -239,7 +239,7 @@ typedef struct cfd_cg_system {
  * the device: x (device, cells) is the starting guess in and the solution
  * out; report (host, 4 doubles, may be NULL) = {iterations, initial residual,
  * final residual, converged}; both residuals are L1 norms as in the
- * reference. Allocates its scratch (two coefficient arrays, five vectors) for
+ * reference. Allocates its scratch (two coefficient arrays, seven vectors) for
  * the call. stream: a cudaStream_t, or NULL for the legacy default stream.
  * Returns after the solve has finished. A wake-map entry >= cells_i*cells_j
  * is refused with CFD_INVALID_ARGUMENT, and x is then left unchanged. */
@@ -250,7 +250,7 @@ cfd_status cfd_cg_solve(const cfd_cg_system* system, double* x, double tolerance
  * application whose memory manager owns the whole device, or a loop that must
  * not block on cudaFree's device-wide synchronisation. No counterpart in the
  * reference. It calls no cudaMalloc, cudaFree or allocating library routine:
- * its scratch is a fixed device array inside this library (3.8 MiB per GPU
+ * its scratch is a fixed device array inside this library (4.75 MiB per GPU
  * that loads it, kept until exit), so blocks are limited to
  * (cells_i+1)*(cells_j+1) <= 65536 nodes; larger ones return
  * CFD_OUT_OF_RANGE. All calls on a device share that array; calls that
@@ -308,16 +308,23 @@ typedef struct cfd_result {
   double alpha_deg;              /* the incidence solved (a sweep's points get theirs here) */
   int continued;                 /* 1: started from the previous sweep point's u and p */
   int error;                     /* CFD_SOLVE_FAILED: why the solve could not start */
+  double mesh_s;                 /* seconds the request's C-grid took to generate (0: cached) */
 } cfd_result;
 
 /* memory_budget_bytes: device memory the resident solves may hold (0: 80 %
  * of the free memory). chunk: iterations per engine step. */
 cfd_status cfd_engine_create(unsigned long long memory_budget_bytes, int chunk, cfd_engine* out);
-/* Queue a request; *id identifies its result. Meshes are generated here. */
+/* Queue a request; *id identifies its result. Its C-grid is generated on the
+ * engine's host worker threads (or taken from the engine's cache), and the
+ * request is admitted once the grid is ready; a grid the generator refuses
+ * makes the request fail (CFD_SOLVE_FAILED, error = the generator's code). */
 cfd_status cfd_engine_submit(cfd_engine e, const cfd_request* request, int* id);
-/* One step: admit what fits, advance every resident solve by up to `chunk`
- * iterations, retire finished ones. active/queued (may be NULL) report the
- * counts afterwards. */
+/* One step: wait for the chunk the previous step launched (setting up the
+ * requests that can join meanwhile), retire finished solves, admit what fits
+ * the memory freed, and launch the next `chunk` iterations of every resident
+ * solve, returning while they run. active/queued (may be NULL) report the
+ * resident solves (those running) and the queued requests afterwards; keep
+ * stepping while either is non-zero. */
 cfd_status cfd_engine_step(cfd_engine e, int* active, int* queued);
 /* post::sweepAngles (src/post/Polar.cpp:36-77): the angles from start to end
  * (a descending sweep when end < start) in steps of |step|, the point count
