@@ -146,6 +146,11 @@ class Forces(C.Structure):
                 ("separation_lower_chord_fraction", C.c_double)]
 
 
+class StreamlineOptions(C.Structure):
+    _fields_ = [("max_steps", C.c_int), ("step_fraction", C.c_double), ("stall_fraction", C.c_double),
+                ("reference_speed", C.c_double), ("trace_backwards", C.c_int)]
+
+
 class CGridOptions(C.Structure):
     _fields_ = [("upstream_chords", C.c_double), ("downstream_chords", C.c_double),
                 ("vertical_chords", C.c_double), ("surface_points", C.c_int),
@@ -177,6 +182,8 @@ _sig("cfd_gpu_set_settings", C.c_int, _P, _P)
 _sig("cfd_gpu_forces", C.c_int, _P, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
      _P, _P, _P)
 _sig("cfd_gpu_dims", C.c_int, _P, _P)
+_sig("cfd_default_streamline_options", None, _P)
+_sig("cfd_gpu_streamlines", C.c_int, _P, _P, C.c_int, _P, _P, _P, C.c_longlong, _P)
 _sig("cfd_gpu_scalars", C.c_int, _P, _P)
 _sig("cfd_gpu_destroy", C.c_int, _P)
 _sig("cfd_default_cgrid_options", None, _P)
@@ -449,6 +456,27 @@ class SimpleSolver:
         _check(_lib.cfd_gpu_forces(self._h, speed, alpha_deg, density, reference_pressure, chord,
                                    C.byref(f), _ptr(cp), _ptr(cf)))
         return f, cp[: f.stations], cf[: f.stations]
+
+    def streamlines(self, seeds, max_steps: int = 4000, step_fraction: float = 0.35,
+                    stall_fraction: float = 1e-4, reference_speed: float = 1.0,
+                    trace_backwards: bool = True):
+        """post::traceStreamlines on the device (cfd_gpu_streamlines): the
+        point count per seed (0 where a seed is dropped) and the curves'
+        points, one after another, as a (total, 2) array."""
+        xy = np.ascontiguousarray(seeds, dtype=np.float64).reshape(-1, 2)
+        n = xy.shape[0]
+        o = StreamlineOptions()
+        _lib.cfd_default_streamline_options(C.byref(o))
+        o.max_steps, o.step_fraction, o.stall_fraction = max_steps, step_fraction, stall_fraction
+        o.reference_speed, o.trace_backwards = reference_speed, 1 if trace_backwards else 0
+        lengths = np.zeros(n, np.int32)
+        total = C.c_longlong()
+        _check(_lib.cfd_gpu_streamlines(self._h, _ptr(xy), n, C.byref(o), _ptr(lengths), None, 0,
+                                        C.byref(total)))
+        pts = np.zeros((max(total.value, 1), 2))
+        _check(_lib.cfd_gpu_streamlines(self._h, _ptr(xy), n, C.byref(o), _ptr(lengths), _ptr(pts),
+                                        total.value, C.byref(total)))
+        return lengths, pts[: total.value]
 
     def scalars(self) -> np.ndarray:
         out = np.zeros(3)

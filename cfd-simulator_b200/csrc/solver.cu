@@ -287,6 +287,8 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     view.partner = partner_;
     if (Status st = buildWallTable(view, m.nodes, &wall_); st != CFD_OK) return st;
   }
+  // node coordinates, for the streamline tracer (copied to the device on first use)
+  if (m.nodes != nullptr) nodes_.assign(m.nodes, m.nodes + 2 * static_cast<std::size_t>(ni) * nj);
   const std::size_t S = static_cast<std::size_t>(std::max(wall_.count(), 1));
 
   // ---- device layout ----
@@ -546,6 +548,7 @@ int Solver::launchSmemBytes(int clusterSize) const {
 
 Solver::~Solver() {
   if (stream_ != nullptr) cudaStreamDestroy(stream_);
+  if (dNodes_ != nullptr) cudaFree(dNodes_);
 }
 
 Status Solver::uploadSettings() {
@@ -919,6 +922,91 @@ Status Solver::readField(int which, double* out) {
   return fail(CFD_OUT_OF_RANGE, "unknown field " + std::to_string(which));
 }
 
+Status Solver::streamlines(const double* seeds, int count, const StreamlineSettings& o, int* lengths,
+                           double* points, long long capacity, long long* total) {
+  if (!initialised_) return fail(CFD_INVALID_ARGUMENT, "initialise() has not been called");
+  if (nodes_.empty()) return fail(CFD_NOT_FOUND, "the mesh was created without node coordinates");
+  if (count < 0 || (count > 0 && seeds == nullptr) || lengths == nullptr) {
+    return fail(CFD_INVALID_ARGUMENT, "seeds and lengths are required");
+  }
+  if (o.maxSteps < 1 || !(o.stepFraction > 0.0)) {
+    return fail(CFD_INVALID_ARGUMENT, "streamline step settings are unusable");  // Streamlines.cpp:101-103
+  }
+  if (count == 0) {
+    if (total != nullptr) *total = 0;
+    return CFD_OK;
+  }
+  if (dNodes_ == nullptr) {
+    CUDA_OR_FAIL(cudaMalloc(reinterpret_cast<void**>(&dNodes_), nodes_.size() * sizeof(double)));
+    CUDA_OR_FAIL(cudaMemcpy(dNodes_, nodes_.data(), nodes_.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  // per call: the seeds, their cells, and both halves of every curve
+  const std::size_t perCurve = 2 * static_cast<std::size_t>(o.maxSteps + 1);
+  const std::size_t bytes = 2 * count * sizeof(double) + count * sizeof(int) + 2 * count * sizeof(int) +
+                            2 * count * perCurve * sizeof(double) + 512;
+  char* scratch = nullptr;
+  CUDA_OR_FAIL(cudaMalloc(reinterpret_cast<void**>(&scratch), bytes));
+  auto release = [&]() { cudaFree(scratch); };
+  double* dSeeds = reinterpret_cast<double*>(scratch);
+  double* dPoints = dSeeds + 2 * count;
+  int* dCells = reinterpret_cast<int*>(dPoints + 2 * count * perCurve);
+  int* dLengths = dCells + count;
+  cudaError_t e = cudaMemcpyAsync(dSeeds, seeds, 2 * count * sizeof(double), cudaMemcpyHostToDevice, stream_);
+  if (e != cudaSuccess) {
+    release();
+    return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  }
+  const Instance& I = view_;
+  if (Status st = launchStreamlines(NI_, NJ_, dNodes_, I.vol, I.acrossJ0, I.u, I.v, count, dSeeds, o, dCells,
+                                    dPoints, dLengths, stream_);
+      st != CFD_OK) {
+    release();
+    return st;
+  }
+  std::vector<int> half(2 * static_cast<std::size_t>(count));
+  std::vector<double> raw(2 * count * perCurve);
+  e = cudaMemcpyAsync(half.data(), dLengths, half.size() * sizeof(int), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(raw.data(), dPoints, raw.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  release();
+  if (e != cudaSuccess) return fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  // Each curve reads in the direction of the flow: the upstream half
+  // reversed, then the downstream half without its repeated seed; a seed
+  // outside the domain or a curve of fewer than 4 points is dropped
+  // (Streamlines.cpp:185-194).
+  long long written = 0;
+  Status status = CFD_OK;
+  for (int s = 0; s < count; ++s) {
+    const int back = half[2 * s], fwd = half[2 * s + 1];
+    const int n = (back + fwd < 4) ? 0 : back + (fwd > 0 ? fwd - 1 : 0);
+    lengths[s] = n;
+    if (n == 0) continue;
+    if (points == nullptr || written + n > capacity) {
+      status = CFD_OUT_OF_RANGE;
+      written += n;
+      continue;
+    }
+    double* out = points + 2 * written;
+    const double* b = raw.data() + (2 * s) * perCurve;
+    const double* f = raw.data() + (2 * s + 1) * perCurve;
+    int k = 0;
+    for (int q = back - 1; q >= 0; --q, ++k) {
+      out[2 * k] = b[2 * q];
+      out[2 * k + 1] = b[2 * q + 1];
+    }
+    for (int q = (fwd > 0 ? 1 : 0); q < fwd; ++q, ++k) {
+      out[2 * k] = f[2 * q];
+      out[2 * k + 1] = f[2 * q + 1];
+    }
+    written += n;
+  }
+  if (total != nullptr) *total = written;
+  if (status != CFD_OK && points != nullptr) return fail(CFD_OUT_OF_RANGE, "points buffer too small for the curves");
+  return CFD_OK;
+}
+
 Status Solver::forces(double speed, double alphaDeg, double density, double referencePressure,
                       double chord, double* out, double* cp, double* cf, int* stations,
                       int* leadingEdge) {
@@ -1131,6 +1219,29 @@ cfd_status cfd_gpu_load_state(cfd_handle h, const double* u, const double* v, co
                               const double* mut, const double* mu_eff) {
   if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
   return h->solver->loadState(u, v, p, mass_flux, k, omega, mut, mu_eff);
+}
+
+void cfd_default_streamline_options(cfd_streamline_options* o) {
+  if (o == nullptr) return;
+  // StreamlineOptions' defaults (include/cfd/post/Streamlines.hpp:16-33)
+  o->max_steps = 4000;
+  o->step_fraction = 0.35;
+  o->stall_fraction = 1e-4;
+  o->reference_speed = 1.0;
+  o->trace_backwards = 1;
+}
+
+cfd_status cfd_gpu_streamlines(cfd_handle h, const double* seeds, int count,
+                               const cfd_streamline_options* options, int* lengths, double* points,
+                               long long capacity, long long* total) {
+  if (cfd_status st = checkHandle(h); st != CFD_OK) return st;
+  cfd_streamline_options o;
+  cfd_default_streamline_options(&o);
+  if (options != nullptr) o = *options;
+  cfdb::StreamlineSettings s{o.max_steps, o.step_fraction,
+                             std::max(o.stall_fraction, 0.0) * std::max(o.reference_speed, 0.0),
+                             o.trace_backwards};
+  return h->solver->streamlines(seeds, count, s, lengths, points, capacity, total);
 }
 
 cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double density,

@@ -17,6 +17,7 @@
 #include "common.hpp"
 #include "forces.hpp"
 #include "instance.hpp"
+#include "streamlines.hpp"
 
 namespace cfdb {
 
@@ -111,6 +112,11 @@ class Solver {
   /// upper-then-lower order.
   Status forces(double speed, double alphaDeg, double density, double referencePressure,
                 double chord, double* out, double* cp, double* cf, int* stations, int* leadingEdge);
+  /// post::traceStreamlines on the current velocity field: lengths[s] points
+  /// per seed (0: dropped), packed in `points` (2 doubles each) up to
+  /// `capacity` points; *total gets the points needed.
+  Status streamlines(const double* seeds, int count, const StreamlineSettings& o, int* lengths,
+                     double* points, long long capacity, long long* total);
 
   int cellsI() const { return NI_; }
   int cellsJ() const { return NJ_; }
@@ -182,6 +188,8 @@ class Solver {
   int* dIterations_{nullptr};
   int historyCapacity_{0};
   double* dWallCentres_{nullptr};
+  std::vector<double> nodes_;   // (x, y) per node, row by row, when the mesh gave them
+  double* dNodes_{nullptr};
   double* dCentroids_{nullptr};
   cudaStream_t stream_{nullptr};
   int clusterSize_{8};

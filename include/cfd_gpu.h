@@ -194,6 +194,29 @@ cfd_status cfd_gpu_forces(cfd_handle h, double speed, double alpha_deg, double d
                           double reference_pressure, double chord, cfd_forces* out, double* cp,
                           double* cf);
 
+/* post::StreamlineOptions (include/cfd/post/Streamlines.hpp:16-33). */
+typedef struct cfd_streamline_options {
+  int max_steps;           /* RK4 steps in each direction, 4000 */
+  double step_fraction;    /* step length / sqrt(cell area), 0.35 */
+  double stall_fraction;   /* stop below this fraction of the reference speed, 1e-4 */
+  double reference_speed;  /* 1.0 */
+  int trace_backwards;     /* 1: trace upstream from each seed too */
+} cfd_streamline_options;
+void cfd_default_streamline_options(cfd_streamline_options* out);
+
+/* post::traceStreamlines (src/post/Streamlines.cpp:80-197) through the
+ * solver's current velocity field, on the device (one thread per seed and
+ * direction; RK4 with the reference's cell location, across the wake cut).
+ * seeds: host (x, y) pairs; options may be NULL for the defaults. lengths
+ * (host, count ints) gets each seed's point count, 0 where the reference
+ * drops the seed (outside the domain, or fewer than 4 points); points (host)
+ * the curves one after another, upstream end first, (x, y) per point, when
+ * `capacity` points fit (else CFD_OUT_OF_RANGE; points may be NULL to ask);
+ * *total (may be NULL) the points needed. Needs mesh nodes. */
+cfd_status cfd_gpu_streamlines(cfd_handle h, const double* seeds, int count,
+                               const cfd_streamline_options* options, int* lengths, double* points,
+                               long long capacity, long long* total);
+
 /* Overwrite the solver state (a warm start, or a state to continue from):
  * u, v, p per cell; mass_flux per face (may be NULL to keep); k, omega, mut
  * per cell (NULL unless SST); mu_eff per cell (may be NULL). */

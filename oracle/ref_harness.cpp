@@ -47,6 +47,7 @@
 #include "cfd/mesh/Mesh.hpp"
 #include "cfd/post/Forces.hpp"
 #include "cfd/post/Polar.hpp"
+#include "cfd/post/Streamlines.hpp"
 #include "cfd/post/SurfaceData.hpp"
 #include "cfd/solver/Gradient.hpp"
 #include "cfd/solver/KOmegaSST.hpp"
@@ -674,6 +675,46 @@ int ref_polar_csv(const char* section, const char* mesh, double reynolds, double
   const std::string text = cfd::post::toCsv(polar);
   if (static_cast<int>(text.size()) <= capacity) std::memcpy(out, text.data(), text.size());
   return static_cast<int>(text.size());
+}
+
+// ----------------------------------------------------------- streamlines ---
+
+/// post::traceStreamlines (Streamlines.cpp:80-197) on the solver's current
+/// field. lengths[s] gets each seed's point count (0 where the seed was
+/// dropped); points the curves one after another while they fit `capacity`
+/// points. Returns the total point count, or -1 on the reference's refusal.
+long long ref_streamlines(void* s, const double* seeds, int count, int maxSteps, double stepFraction,
+                          double stallFraction, double referenceSpeed, int traceBackwards, int* lengths,
+                          double* points, long long capacity) {
+  RefSolver* r = static_cast<RefSolver*>(s);
+  cfd::post::StreamlineOptions o;
+  for (int k = 0; k < count; ++k) o.seeds.push_back(Vec2{seeds[2 * k], seeds[2 * k + 1]});
+  o.maxSteps = maxSteps;
+  o.stepFraction = stepFraction;
+  o.stallFraction = stallFraction;
+  o.referenceSpeed = referenceSpeed;
+  o.traceBackwards = traceBackwards != 0;
+  // which seeds survive: the reference returns only the kept curves, in seed
+  // order, so a seed's curve is matched by tracing it alone
+  long long total = 0;
+  for (int k = 0; k < count; ++k) {
+    cfd::post::StreamlineOptions one = o;
+    one.seeds = {o.seeds[static_cast<std::size_t>(k)]};
+    auto lines = cfd::post::traceStreamlines(r->mesh->mesh, r->solver->field(), one);
+    if (!lines) {
+      g_error = lines.error().format();
+      return -1;
+    }
+    const std::size_t n = lines.value().empty() ? 0 : lines.value().front().size();
+    lengths[k] = static_cast<int>(n);
+    for (std::size_t q = 0; q < n; ++q, ++total) {
+      if (total < capacity) {
+        points[2 * total] = lines.value().front()[q].x;
+        points[2 * total + 1] = lines.value().front()[q].y;
+      }
+    }
+  }
+  return total;
 }
 
 }  // extern "C"

@@ -70,6 +70,7 @@ def lib():
             ("ref_green_gauss", None, [P_] * 3),
             ("ref_forces", i, [P_, d, d, d, d, d, P_, P_]),
             ("ref_sweep_angles", i, [d, d, d, P_, i]),
+            ("ref_streamlines", C.c_longlong, [P_, P_, i, i, d, d, d, i, P_, P_, C.c_longlong]),
             ("ref_polar_csv", i, [C.c_char_p, C.c_char_p, d, d, d, d, i, i, P_, C.c_char_p, i]),
         ]:
             fn = getattr(_lib, name)
@@ -205,6 +206,22 @@ class RefSolver:
 
     def keep_momentum_diagonal(self):
         lib().ref_solver_keep_momentum_diagonal(self._h)
+
+    def streamlines(self, seeds, max_steps=4000, step_fraction=0.35, stall_fraction=1e-4,
+                    reference_speed=1.0, trace_backwards=True):
+        """post::traceStreamlines on the current field: (lengths per seed,
+        points (total, 2)); a dropped seed has length 0."""
+        xy = np.ascontiguousarray(seeds, dtype=np.float64).reshape(-1, 2)
+        n = xy.shape[0]
+        lengths = np.zeros(n, np.int32)
+        args = (self._h, _p(xy), n, max_steps, step_fraction, stall_fraction, reference_speed,
+                1 if trace_backwards else 0, _p(lengths))
+        total = lib().ref_streamlines(*args, None, 0)
+        if total < 0:
+            raise ValueError(lib().ref_last_error().decode())
+        pts = np.zeros((max(total, 1), 2))
+        lib().ref_streamlines(*args, _p(pts), total)
+        return lengths, pts[:total]
 
     def sst_scalars(self):
         out = np.zeros(5)
