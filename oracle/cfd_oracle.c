@@ -349,16 +349,23 @@ static void wall_distances(or_solver* s) {
     for (int c = 0; c < s->N; ++c) s->wd[c] = far;
     return;
   }
+  /* the wall faces in ascending order, then the same scan over them */
+  int* wall = (int*)malloc(sizeof(int) * (size_t)walls);
+  int n = 0;
+  for (int f = 0; f < s->F; ++f) {
+    if (s->kind[f] == K_WALL) wall[n++] = f;
+  }
   for (int c = 0; c < s->N; ++c) {
     const double cx = m->centroid[2 * c], cy = m->centroid[2 * c + 1];
     double best = 1.7976931348623157e308;
-    for (int f = 0; f < s->F; ++f) {
-      if (s->kind[f] != K_WALL) continue;
+    for (int k = 0; k < walls; ++k) {
+      const int f = wall[k];
       const double dx = cx - m->face_centre[2 * f], dy = cy - m->face_centre[2 * f + 1];
       best = mn(best, dx * dx + dy * dy);
     }
     s->wd[c] = sqrt(best);
   }
+  free(wall);
 }
 
 static double wall_omega(double nu, double distance, double energy) {
