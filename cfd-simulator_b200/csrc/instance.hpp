@@ -55,6 +55,7 @@ constexpr int kFlagGlobalCg = 1;
 constexpr int kFlagPlainWavefront = 2;
 constexpr int kFlagSequentialRows = 4;
 constexpr int kFlagTwoReductionCg = 8;
+constexpr int kFlagOnePassCg = 16;
 
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {

@@ -604,6 +604,7 @@ DEV void gsRowScanSweeps(const Instance& I, int sweeps, const SysView<T>& y, T* 
   for (int sweep = 0; sweep < sweeps; ++sweep) {
     for (int j = 0; j < I.NJ; ++j) {
       gsRow(I, j, y, rowNew, rowPrev, sc);
+      prefetchRow(I, (j + 1 < I.NJ) ? j + 1 : 0, y);
       __syncthreads();
     }
   }
@@ -618,6 +619,21 @@ DEV void gsRowScanSweeps(const Instance& I, int sweeps, const SysView<T>& y, T* 
 /// j+2, sweep s+1 row j-2). Every CTA of the cluster joins each step's
 /// barrier. Same arithmetic as gsRowScanSweeps, NJ + 2 (sweeps - 1) steps
 /// instead of sweeps * NJ.
+/// Bring row j's coefficients and right-hand side (fixed during the sweeps)
+/// towards this SM's L1 ahead of its scan, one prefetch per 128-byte line,
+/// spread over the CTA's threads. A hint only: it changes no value.
+template <typename T>
+DEV void prefetchRow(const Instance& I, int j, const SysView<T>& y) {
+  if (j < 0 || j >= I.NJ) return;
+  constexpr int perLine = 128 / static_cast<int>(sizeof(T));
+  const int lines = (I.NI + perLine - 1) / perLine;
+  const T* arrays[6] = {y.D, y.S, y.N, y.W, y.E, y.b};
+  for (int q = threadIdx.x; q < 6 * lines; q += blockDim.x) {
+    const T* line = arrays[q / lines] + static_cast<long long>(j) * I.NI + (q % lines) * perLine;
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(line));
+  }
+}
+
 template <typename T>
 DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, const SysView<T>& kSys,
                             const SysView<T>& wSys, T* smem) {
@@ -630,9 +646,11 @@ DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, const SysVie
   T* rowPrev = smem + I.NI;
   T* sc = smem + 2 * I.NI;
   const int steps = I.NJ + 2 * (sweeps - 1);
+  if (active) prefetchRow(I, -2 * s, y);
   for (int step = 0; step < steps; ++step) {
     const int j = step - 2 * s;
     if (active && j >= 0 && j < I.NJ) gsRow(I, j, y, rowNew, rowPrev, sc);
+    if (active) prefetchRow(I, j + 1, y);  // the next step's row, over the barrier
     t.cl.sync();
   }
 }
@@ -1279,6 +1297,15 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
   int iterations = 0;
   int cur = 0;
   const int op3[3] = {kSum, kSum, kSum};
+  // Restrict-qualified views: no store of the loop below can alias a load of
+  // it, so the loads of the next cells may be issued ahead of the stores of
+  // the current ones (the loop is latency-bound without that).
+  const double* __restrict__ pD = I.pD;
+  const double* __restrict__ pN = I.pN;
+  const double* __restrict__ pE = I.pE;
+  const int* __restrict__ wake = I.acrossJ0;
+  double* __restrict__ xv = I.x;
+  double* __restrict__ pv = I.cgp;
   for (int iter = 0; iter < I.cgMax; ++iter) {
     const double* __restrict__ r = rB[cur];
     const double* __restrict__ w = wB[cur];
@@ -1288,25 +1315,27 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
     double* __restrict__ sn = sB[cur ^ 1];
     const double alpha = k.alpha, beta = k.beta;
     double sums[3] = {0.0, 0.0, 0.0};
+    // the next u of a cell from its r, w and s of this iteration
+    auto uAt = [&](int n) {
+      const double s2 = w[n] + beta * sv[n];
+      return precondition(r[n] - alpha * s2, pD[n]);
+    };
+#pragma unroll 2
     for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
       const int i = c % NI, j = c / NI;
-      auto uAt = [&](int n) {
-        const double s2 = w[n] + beta * sv[n];
-        return precondition(r[n] - alpha * s2, I.pD[n]);
-      };
-      const double dg = I.pD[c];
-      const double pc = precondition(r[c], dg) + beta * I.cgp[c];
+      const double dg = pD[c];
+      const double pc = precondition(r[c], dg) + beta * pv[c];
       const double sc = w[c] + beta * sv[c];
-      I.x[c] += alpha * pc;
+      xv[c] += alpha * pc;
       const double rc = r[c] - alpha * sc;
       const double un = precondition(rc, dg);
       double y = dg * un;
-      const int nS = (j > 0) ? c - NI : I.acrossJ0[i];
-      if (nS >= 0) y += I.pN[j * NI + i] * uAt(nS);
-      if (j < NJ - 1) y += I.pN[(j + 1) * NI + i] * uAt(c + NI);
-      if (i > 0) y += I.pE[j * (NI + 1) + i] * uAt(c - 1);
-      if (i < NI - 1) y += I.pE[j * (NI + 1) + i + 1] * uAt(c + 1);
-      I.cgp[c] = pc;
+      const int nS = (j > 0) ? c - NI : wake[i];
+      if (nS >= 0) y += pN[j * NI + i] * uAt(nS);
+      if (j < NJ - 1) y += pN[(j + 1) * NI + i] * uAt(c + NI);
+      if (i > 0) y += pE[j * (NI + 1) + i] * uAt(c - 1);
+      if (i < NI - 1) y += pE[j * (NI + 1) + i + 1] * uAt(c + 1);
+      pv[c] = pc;
       sn[c] = sc;
       rn[c] = rc;
       wn[c] = y;
@@ -1315,6 +1344,148 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
       sums[2] += fabs(rc);
     }
     cur ^= 1;
+    teamReduce(t, sh, sums, op3);
+    iterations = iter + 1;
+    if (!cgNext(I, k, sums, initial)) break;
+  }
+  return iterations;
+}
+
+/// Shared memory of cgGlobalSplit, in doubles: each CTA's boundary rows'
+/// r, w and s for the neighbouring CTAs (two parities x two rows x three
+/// values x NI), the next u of the two rows bordering its band (2 x NI), and
+/// the next u of its own band (the largest band's cells).
+__host__ __device__ inline long long cgSplitSmemDoubles(int NI, int NJ, int R) {
+  return 14LL * NI + cgSmemStride(NI, NJ, R);
+}
+
+/// The single-reduction PCG of cgGlobal in two passes per iteration, for
+/// bands in global memory, with r, w and s held once: the first pass forms
+/// each own cell's p, s, x, r and next u in place (u stored), and the next u
+/// of the two rows bordering the band from the r, w and s the neighbouring
+/// CTAs exported for them (u in shared memory); after a block barrier the
+/// second forms w' = A u' from them and exports the band's first and last
+/// rows' new r, w and s to this CTA's shared memory (double-buffered by
+/// iteration parity, read by the neighbours through DSMEM after the
+/// iteration's reduction). Each pass has few independent loads per cell, so
+/// they overlap across cells; the one-pass form's neighbour recomputation
+/// (four loads per neighbour, three vectors double-buffered) leaves it
+/// latency-bound and 30 % larger in L2. The same expressions in the same cell
+/// order as cgGlobal and cgShared, so the same bits.
+DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double gamma) {
+  const int NI = I.NI, NJ = I.NJ;
+  const int R = static_cast<int>(t.R), rank = static_cast<int>(t.rank);
+  const double* __restrict__ pD = I.pD;
+  const double* __restrict__ pN = I.pN;
+  const double* __restrict__ pE = I.pE;
+  const int* __restrict__ wake = I.acrossJ0;
+  double* __restrict__ xv = I.x;
+  double* __restrict__ pv = I.cgp;
+  double* __restrict__ rv = I.r;
+  double* __restrict__ wv = I.q;
+  double* __restrict__ sv = I.d1;
+  // exports: [parity][row: 0 first, 1 last][value: r, w, s][i]; then the halo
+  // u and the band's own u (cell c at c - c0)
+  double* ex = dyn;
+  double* halo = dyn + 12 * NI;  // [0, NI): row j0 - 1; [NI, 2 NI): row j1
+  double* __restrict__ ub = dyn + 14 * NI;  // cell c at ub[c - c0]
+  const int c0 = t.c0;
+  const double* below = (rank > 0) ? t.cl.map_shared_rank(ex, rank - 1) : nullptr;
+  const double* above = (rank < R - 1) ? t.cl.map_shared_rank(ex, rank + 1) : nullptr;
+  auto slot = [NI](int parity, int row, int value) { return ((parity * 2 + row) * 3 + value) * NI; };
+  const int j0 = t.c0 / NI, j1 = t.c1 / NI;
+  auto exportRows = [&](int parity, int c, double r, double w, double s) {
+    const int i = c % NI, j = c / NI;
+    if (j == j0) {
+      ex[slot(parity, 0, 0) + i] = r;
+      ex[slot(parity, 0, 1) + i] = w;
+      ex[slot(parity, 0, 2) + i] = s;
+    }
+    if (j == j1 - 1) {
+      ex[slot(parity, 1, 0) + i] = r;
+      ex[slot(parity, 1, 1) + i] = w;
+      ex[slot(parity, 1, 2) + i] = s;
+    }
+  };
+  // w0 = A u0 (u0 from b, stable since the start's reduction); p = s = 0
+  double acc[1] = {0.0};
+  const int op1[1] = {kSum};
+  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+    const int i = c % NI, j = c / NI;
+    auto uAt = [&](int n) { return precondition(rv[n], pD[n]); };
+    const double un = precondition(rv[c], pD[c]);
+    double y = pD[c] * un;
+    const int nS = (j > 0) ? c - NI : wake[i];
+    if (nS >= 0) y += pN[j * NI + i] * uAt(nS);
+    if (j < NJ - 1) y += pN[(j + 1) * NI + i] * uAt(c + NI);
+    if (i > 0) y += pE[j * (NI + 1) + i] * uAt(c - 1);
+    if (i < NI - 1) y += pE[j * (NI + 1) + i + 1] * uAt(c + 1);
+    acc[0] += y * un;
+    wv[c] = y;
+    pv[c] = 0.0;
+    sv[c] = 0.0;
+    exportRows(0, c, rv[c], y, 0.0);
+  }
+  teamReduce(t, sh, acc, op1);
+  if (!(fabs(acc[0]) > 0.0)) return 0;
+  CgScalars k;
+  k.alpha = gamma / acc[0];
+  k.gamma = gamma;
+  int iterations = 0;
+  const int op3[3] = {kSum, kSum, kSum};
+  for (int iter = 0; iter < I.cgMax; ++iter) {
+    const int par = iter & 1;
+    const double alpha = k.alpha, beta = k.beta;
+    double sums[3] = {0.0, 0.0, 0.0};
+    // the bordering rows' next u, from the r, w and s their CTAs exported
+    for (int q = t.tid; q < 2 * NI; q += t.T) {
+      const bool low = q < NI;
+      const double* src = low ? below : above;
+      if (src == nullptr) continue;
+      const int i = low ? q : q - NI;
+      const int row = low ? 1 : 0;  // the CTA below exports its last row, the one above its first
+      const double rn = src[slot(par, row, 0) + i];
+      const double wn = src[slot(par, row, 1) + i];
+      const double sn = src[slot(par, row, 2) + i];
+      const int n = (low ? (j0 - 1) : j1) * NI + i;
+      const double s2 = wn + beta * sn;
+      halo[q] = precondition(rn - alpha * s2, pD[n]);
+    }
+    // pass 1: own cells
+#pragma unroll 4
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const double dg = pD[c];
+      const double rc0 = rv[c];
+      const double pc = precondition(rc0, dg) + beta * pv[c];
+      const double sc = wv[c] + beta * sv[c];
+      xv[c] += alpha * pc;
+      const double rc = rc0 - alpha * sc;
+      const double un = precondition(rc, dg);
+      pv[c] = pc;
+      sv[c] = sc;
+      rv[c] = rc;
+      ub[c - c0] = un;
+      sums[0] += rc * un;
+      sums[2] += fabs(rc);
+    }
+    __syncthreads();
+    // pass 2: w' = A u', and the boundary rows' new r, w and s for the neighbours
+#pragma unroll 4
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      const int i = c % NI, j = c / NI;
+      const double dg = pD[c];
+      const int m = c - c0;
+      const double un = ub[m];
+      double y = dg * un;
+      if (j > 0) y += pN[j * NI + i] * ((j == j0) ? halo[i] : ub[m - NI]);
+      else if (wake[i] >= 0) y += pN[i] * ub[wake[i] - c0];
+      if (j < NJ - 1) y += pN[(j + 1) * NI + i] * ((j + 1 == j1) ? halo[NI + i] : ub[m + NI]);
+      if (i > 0) y += pE[j * (NI + 1) + i] * ub[m - 1];
+      if (i < NI - 1) y += pE[j * (NI + 1) + i + 1] * ub[m + 1];
+      wv[c] = y;
+      sums[1] += y * un;
+      if (j == j0 || j == j1 - 1) exportRows(par ^ 1, c, rv[c], y, sv[c]);
+    }
     teamReduce(t, sh, sums, op3);
     iterations = iter + 1;
     if (!cgNext(I, k, sums, initial)) break;
@@ -1505,6 +1676,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
         cgIters = cgTwoReductions(I, t, sh, initial, rz);
       } else if (initial > 0.0 && cgInShared) {
         cgIters = cgShared(I, t, sh, dyn, initial, rz);
+      } else if (initial > 0.0 && !(flags & kFlagOnePassCg) && I.NJ >= static_cast<int>(t.R) &&
+                 cgSplitSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes) {
+        cgIters = cgGlobalSplit(I, t, sh, dyn, initial, rz);
       } else if (initial > 0.0) {
         cgIters = cgGlobal(I, t, sh, initial, rz);
       }
@@ -1666,19 +1840,25 @@ int kernelFlags() {
   // Implementation choices for tuning comparisons: bit 0 keeps the pressure
   // CG in global memory, bit 1 uses the plain wavefront sweeps, bit 2 runs
   // the k/omega row sweeps one after another instead of pipelined across
-  // CTAs (these three give identical results); bit 3 runs the reference's
-  // two-reduction CG instead of the single-reduction one (the same to
-  // rounding).
+  // CTAs, bit 4 runs the global-memory CG in one pass per iteration
+  // instead of two (these four give identical results); bit 3 runs the
+  // reference's two-reduction CG instead of the single-reduction one (the
+  // same to rounding).
   const char* env = std::getenv("CFD_KERNEL_FLAGS");
   return (env != nullptr) ? std::atoi(env) : 0;
 }
 
 int cgSharedBytes(int NI, int NJ, int clusterSize) {
-  // The k/omega row sweeps keep two rows and the scan's warp totals.
+  // The k/omega row sweeps keep two rows and the scan's warp totals; the
+  // pressure CG its band (cgShared) or, where that does not fit, the
+  // exported boundary rows of the two-pass global-memory form.
   const long long wave = (2LL * NI + 64) * 8;
   long long bytes = 0;
   if (NJ >= clusterSize) bytes = cgSmemDoubles(NI, NJ, clusterSize) * 8;
   if (bytes > kMaxCgSharedBytes) bytes = 0;
+  if (bytes == 0 && NJ >= clusterSize && cgSplitSmemDoubles(NI, NJ, clusterSize) * 8 <= kMaxCgSharedBytes) {
+    bytes = cgSplitSmemDoubles(NI, NJ, clusterSize) * 8;
+  }
   if (bytes < wave && wave <= kMaxCgSharedBytes) bytes = wave;
   return static_cast<int>(bytes);
 }
