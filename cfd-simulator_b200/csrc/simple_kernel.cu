@@ -1355,6 +1355,9 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
 /// r, w and s for the neighbouring CTAs (two parities x two rows x three
 /// values x NI), the next u of the two rows bordering its band (2 x NI), and
 /// the next u of its own band (the largest band's cells).
+/// Cells per software-pipeline group in cgGlobalSplit's passes.
+constexpr int kCgPair = 2;
+
 __host__ __device__ inline long long cgSplitSmemDoubles(int NI, int NJ, int R) {
   return 14LL * NI + cgSmemStride(NI, NJ, R);
 }
@@ -1390,6 +1393,8 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
   double* halo = dyn + 12 * NI;  // [0, NI): row j0 - 1; [NI, 2 NI): row j1
   double* __restrict__ ub = dyn + 14 * NI;  // cell c at ub[c - c0]
   const int c0 = t.c0;
+  // cells of this thread in the band: c0 + tid + k T, k < own
+  const int own = (t.c1 - t.c0 > t.tid) ? (t.c1 - t.c0 - t.tid + t.T - 1) / t.T : 0;
   const double* below = (rank > 0) ? t.cl.map_shared_rank(ex, rank - 1) : nullptr;
   const double* above = (rank < R - 1) ? t.cl.map_shared_rank(ex, rank + 1) : nullptr;
   auto slot = [NI](int parity, int row, int value) { return ((parity * 2 + row) * 3 + value) * NI; };
@@ -1451,40 +1456,97 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
       const double s2 = wn + beta * sn;
       halo[q] = precondition(rn - alpha * s2, pD[n]);
     }
-    // pass 1: own cells
-#pragma unroll 4
-    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-      const double dg = pD[c];
-      const double rc0 = rv[c];
-      const double pc = precondition(rc0, dg) + beta * pv[c];
-      const double sc = wv[c] + beta * sv[c];
-      xv[c] += alpha * pc;
-      const double rc = rc0 - alpha * sc;
-      const double un = precondition(rc, dg);
-      pv[c] = pc;
-      sv[c] = sc;
-      rv[c] = rc;
-      ub[c - c0] = un;
-      sums[0] += rc * un;
-      sums[2] += fabs(rc);
+    // pass 1: own cells. Software-pipelined by hand: the next pair of cells'
+    // loads are issued before this pair's arithmetic (the division's slow
+    // path otherwise keeps the compiler from hoisting them), so two pairs of
+    // loads are in flight per thread. Indices past the band are clamped to its
+    // last cell and their values discarded; cells keep their order per thread.
+    {
+      double nD[kCgPair], nR[kCgPair], nP[kCgPair], nW[kCgPair], nS[kCgPair], nX[kCgPair];
+      auto load = [&](int k, int u) {
+        const int c = min(t.c0 + t.tid + k * t.T, t.c1 - 1);
+        nD[u] = pD[c]; nR[u] = rv[c]; nP[u] = pv[c]; nW[u] = wv[c]; nS[u] = sv[c]; nX[u] = xv[c];
+      };
+#pragma unroll
+      for (int u = 0; u < kCgPair; ++u) load(u, u);
+      for (int k = 0; k < own; k += kCgPair) {
+        double cD[kCgPair], cR[kCgPair], cP[kCgPair], cW[kCgPair], cS[kCgPair], cX[kCgPair];
+#pragma unroll
+        for (int u = 0; u < kCgPair; ++u) {
+          cD[u] = nD[u]; cR[u] = nR[u]; cP[u] = nP[u]; cW[u] = nW[u]; cS[u] = nS[u]; cX[u] = nX[u];
+        }
+        if (k + kCgPair < own) {
+#pragma unroll
+          for (int u = 0; u < kCgPair; ++u) load(k + kCgPair + u, u);
+        }
+#pragma unroll
+        for (int u = 0; u < kCgPair; ++u) {
+          if (k + u >= own) break;
+          const int c = t.c0 + t.tid + (k + u) * t.T;
+          const double dg = cD[u];
+          const double rc0 = cR[u];
+          const double pc = precondition(rc0, dg) + beta * cP[u];
+          const double sc = cW[u] + beta * cS[u];
+          xv[c] = cX[u] + alpha * pc;
+          const double rc = rc0 - alpha * sc;
+          const double un = precondition(rc, dg);
+          pv[c] = pc;
+          sv[c] = sc;
+          rv[c] = rc;
+          ub[c - c0] = un;
+          sums[0] += rc * un;
+          sums[2] += fabs(rc);
+        }
+      }
     }
     __syncthreads();
-    // pass 2: w' = A u', and the boundary rows' new r, w and s for the neighbours
-#pragma unroll 4
-    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-      const int i = c % NI, j = c / NI;
-      const double dg = pD[c];
-      const int m = c - c0;
-      const double un = ub[m];
-      double y = dg * un;
-      if (j > 0) y += pN[j * NI + i] * ((j == j0) ? halo[i] : ub[m - NI]);
-      else if (wake[i] >= 0) y += pN[i] * ub[wake[i] - c0];
-      if (j < NJ - 1) y += pN[(j + 1) * NI + i] * ((j + 1 == j1) ? halo[NI + i] : ub[m + NI]);
-      if (i > 0) y += pE[j * (NI + 1) + i] * ub[m - 1];
-      if (i < NI - 1) y += pE[j * (NI + 1) + i + 1] * ub[m + 1];
-      wv[c] = y;
-      sums[1] += y * un;
-      if (j == j0 || j == j1 - 1) exportRows(par ^ 1, c, rv[c], y, sv[c]);
+    // pass 2: w' = A u', and the boundary rows' new r, w and s for the
+    // neighbours; the coefficient loads pipelined as in pass 1 (every face
+    // index is in range for any cell, so they are loaded unconditionally).
+    {
+      double nD[kCgPair], nNs[kCgPair], nNn[kCgPair], nEw[kCgPair], nEe[kCgPair];
+      int nWk[kCgPair];
+      auto load = [&](int k, int u) {
+        const int c = min(t.c0 + t.tid + k * t.T, t.c1 - 1);
+        const int i = c % NI, j = c / NI;
+        nD[u] = pD[c];
+        nNs[u] = pN[j * NI + i];
+        nNn[u] = pN[(j + 1) * NI + i];
+        nEw[u] = pE[j * (NI + 1) + i];
+        nEe[u] = pE[j * (NI + 1) + i + 1];
+        nWk[u] = wake[i];
+      };
+#pragma unroll
+      for (int u = 0; u < kCgPair; ++u) load(u, u);
+      for (int k = 0; k < own; k += kCgPair) {
+        double cD[kCgPair], cNs[kCgPair], cNn[kCgPair], cEw[kCgPair], cEe[kCgPair];
+        int cWk[kCgPair];
+#pragma unroll
+        for (int u = 0; u < kCgPair; ++u) {
+          cD[u] = nD[u]; cNs[u] = nNs[u]; cNn[u] = nNn[u]; cEw[u] = nEw[u]; cEe[u] = nEe[u]; cWk[u] = nWk[u];
+        }
+        if (k + kCgPair < own) {
+#pragma unroll
+          for (int u = 0; u < kCgPair; ++u) load(k + kCgPair + u, u);
+        }
+#pragma unroll
+        for (int u = 0; u < kCgPair; ++u) {
+          if (k + u >= own) break;
+          const int c = t.c0 + t.tid + (k + u) * t.T;
+          const int i = c % NI, j = c / NI;
+          const int m = c - c0;
+          const double un = ub[m];
+          double y = cD[u] * un;
+          if (j > 0) y += cNs[u] * ((j == j0) ? halo[i] : ub[m - NI]);
+          else if (cWk[u] >= 0) y += cNs[u] * ub[cWk[u] - c0];
+          if (j < NJ - 1) y += cNn[u] * ((j + 1 == j1) ? halo[NI + i] : ub[m + NI]);
+          if (i > 0) y += cEw[u] * ub[m - 1];
+          if (i < NI - 1) y += cEe[u] * ub[m + 1];
+          wv[c] = y;
+          sums[1] += y * un;
+          if (j == j0 || j == j1 - 1) exportRows(par ^ 1, c, rv[c], y, sv[c]);
+        }
+      }
     }
     teamReduce(t, sh, sums, op3);
     iterations = iter + 1;
