@@ -432,7 +432,7 @@ struct Engine {
     q.submitted = now();
     q.sweep = s.sweep;
     q.point = next;
-    const bool cold = !sw.continued || (s.retried && status == CFD_SOLVE_DIVERGED);
+    const bool cold = !sw.continued || (s.retried && status == CFD_SOLVE_DIVERGED) || status == CFD_SOLVE_FAILED;
     if (!cold) {
       auto warm = std::make_shared<WarmStart>();
       const std::size_t n = static_cast<std::size_t>(s.solver->cells());
@@ -508,10 +508,11 @@ struct Engine {
     }
   }
 
-  void finish(Slot& s, int status, const double* mon) {
+  void finish(Slot& s, int status, const double* mon, Status error = CFD_OK) {
     cfd_result r{};
     r.id = s.id;
     r.status = status;
+    r.error = error;
     r.iterations = s.iterations;
     r.retried_cold = s.retried ? 1 : 0;
     r.continued = s.continued ? 1 : 0;
@@ -527,7 +528,7 @@ struct Engine {
     r.separation_lower_chord_fraction = -1.0;
     std::vector<double> cp(static_cast<std::size_t>(std::max(s.solver->wallStations(), 1)));
     int stations = 0;
-    if (status != CFD_SOLVE_DIVERGED &&
+    if (status != CFD_SOLVE_DIVERGED && status != CFD_SOLVE_FAILED &&
         s.solver->forces(s.request.speed, s.request.alpha_deg, s.request.density, 0.0, 1.0, f, cp.data(),
                          nullptr, &stations, nullptr) == CFD_OK) {
       cp.resize(static_cast<std::size_t>(stations));
@@ -631,14 +632,20 @@ struct Engine {
     for (int k = 0; k < n; ++k) {
       Slot& s = *active[k];
       const double* st = status.data() + static_cast<std::size_t>(k) * per;
-      int ran = 0;
-      std::memcpy(&ran, st + static_cast<std::size_t>(chunk) * kMonSlots, sizeof(int));
+      int words[2] = {0, 0};  // iterations, fault word
+      std::memcpy(words, st + static_cast<std::size_t>(chunk) * kMonSlots, sizeof(words));
+      const int ran = words[0];
       s.iterations += ran;
       const double* mon = st + static_cast<std::size_t>(std::max(ran, 1) - 1) * kMonSlots;
       const double a = mon[kMonContinuity], b = mon[kMonMomX], c = mon[kMonMomY];
       const bool finite = std::isfinite(a) && std::isfinite(b) && std::isfinite(c);
       int outcome = -1;
-      if (!finite) {
+      Status error = CFD_OK;
+      if (words[1] != 0) {
+        // a bounded wait in the kernel gave up: the launch's values are not valid
+        error = launchFault(words[1]);
+        outcome = CFD_SOLVE_FAILED;
+      } else if (!finite) {
         if (!s.retried) {
           // RetryCold: restart once from the freestream
           s.retried = true;
@@ -656,7 +663,7 @@ struct Engine {
         outcome = CFD_SOLVE_ITERATION_LIMIT;
       }
       if (outcome >= 0) {
-        finish(s, outcome, mon);
+        finish(s, outcome, mon, error);
         if (s.sweep >= 0) advanceSweep(s, outcome);
         used -= s.bytes;
       } else {

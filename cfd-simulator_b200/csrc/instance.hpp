@@ -56,6 +56,11 @@ constexpr int kFlagPlainWavefront = 2;
 constexpr int kFlagSequentialRows = 4;
 constexpr int kFlagTwoReductionCg = 8;
 constexpr int kFlagOnePassCg = 16;
+constexpr int kFlagBarrierSweeps = 32;
+constexpr int kFlagChainWaitTest = 64;  // tests only: a chained stage also waits for a count nothing sets
+
+// Fault codes a launch leaves in iterations[1] (bits, or-ed together).
+constexpr int kFaultChainWait = 1;  // a chained k/omega sweep stage gave up waiting for its neighbour
 
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {
@@ -146,7 +151,8 @@ struct Instance {
 
   // ---- outputs ----
   double* history;   // kMonSlots doubles per iteration of the launch
-  int* iterations;   // iterations completed by the launch
+  int* iterations;   // iterations completed by the launch, then the launch's fault
+                     // word (iterations[1]: nonzero when a bounded wait gave up)
 
   // ---- mixed form ----
   Multigrid mg;

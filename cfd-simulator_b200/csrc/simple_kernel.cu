@@ -521,19 +521,21 @@ DEV void blockAffineExclusiveScan(T& p, T& q, T* sc) {
 /// first. A cell with a_P = 0 keeps its value (p = x, q = 0). This is the
 /// reference's sweep map; only the rounding differs from cell-by-cell order.
 ///
-/// Run by every thread of one CTA; rowPrev holds row j-1's new values and
-/// receives row j's. Needs NI <= 8 * blockDim.x. Ends without a barrier after
-/// the row is published (the caller synchronises before the next row).
+/// Run by every thread of one CTA; rowPrev holds row j-1's new values,
+/// oldRow and northRow rows j and j+1 as the previous sweep left them (the
+/// unknowns themselves, or a copy). Needs NI <= 8 * blockDim.x. Leaves row
+/// j's new values in rowNew and ends with a barrier; the caller publishes.
 template <typename T>
 struct SysView {
   const T *D, *S, *N, *W, *E, *b;
   T* x;
 };
 
+/// The row solve for any cells per thread (up to 8), loading as it goes.
 template <typename T>
-DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowPrev, T* sc) {
+DEV void gsRowSolveAny(const Instance& I, int j, const SysView<T>& y, const T* oldRow, const T* northRow, T* rowNew,
+                       const T* rowPrev, T* sc) {
   const T *D = y.D, *cS = y.S, *cN = y.N, *cW = y.W, *cE = y.E, *b = y.b;
-  T* x = y.x;
   const int NI = I.NI, NJ = I.NJ;
   const int nt = blockDim.x;
   const int per = (NI + nt - 1) / nt;  // contiguous cells per thread
@@ -554,7 +556,7 @@ DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowP
       const int c = j * NI + i;
       const T d = D[c];
       if (!(fabs(d) > T(0))) {
-        pv[e] = x[c];
+        pv[e] = oldRow[i];
         qv[e] = T(0);
       } else {
         T off = T(0);
@@ -562,10 +564,10 @@ DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowP
           off += cS[c] * rowPrev[i];
         } else {
           const int a = I.acrossJ0[i];
-          if (a >= 0) off += cS[c] * ((a < i) ? rowNew[a] : x[a]);
+          if (a >= 0) off += cS[c] * ((a < i) ? rowNew[a] : oldRow[a]);
         }
-        if (i < NI - 1) off += cE[c] * x[c + 1];
-        if (j < NJ - 1) off += cN[c] * x[c + NI];
+        if (i < NI - 1) off += cE[c] * oldRow[i + 1];
+        if (j < NJ - 1) off += cN[c] * northRow[i];
         pv[e] = (b[c] - off) / d;
         qv[e] = (i > 0) ? -cW[c] / d : T(0);
       }
@@ -584,11 +586,116 @@ DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowP
     __syncthreads();
     if (hi > lo) carry = rowNew[hi - 1];
   }
-  // Publish row j: global memory (east/north reads of later rows and the
-  // next sweep) and rowPrev (the south values of row j + 1). Every read of
-  // this row's old values and of rowPrev happened before the scan's barriers
-  // above.
-  for (int i = threadIdx.x; i < NI; i += nt) {
+}
+
+/// The row solve for at most MAXPER cells per thread. Every operand of the
+/// thread's cells is loaded before any is used (indices clamped into the row;
+/// values of cells outside it are never used), so the loads overlap instead
+/// of waiting behind the branch on the diagonal.
+template <typename T, int MAXPER>
+DEV void gsRowSolveN(const Instance& I, int j, const SysView<T>& y, const T* oldRow, const T* northRow, T* rowNew,
+                     const T* rowPrev, T* sc) {
+  const T* __restrict__ D = y.D;
+  const T* __restrict__ cS = y.S;
+  const T* __restrict__ cN = y.N;
+  const T* __restrict__ cW = y.W;
+  const T* __restrict__ cE = y.E;
+  const T* __restrict__ b = y.b;
+  const int NI = I.NI, NJ = I.NJ;
+  const int nt = blockDim.x;
+  const int per = (NI + nt - 1) / nt;  // contiguous cells per thread
+  const int i0 = threadIdx.x * per;
+  const bool hasNorth = j < NJ - 1;
+  const long long rowBase = static_cast<long long>(j) * NI;
+  T dv[MAXPER], sv[MAXPER], ev[MAXPER], nv[MAXPER], wv[MAXPER], bv[MAXPER];
+  T oldI[MAXPER], oldE[MAXPER], northI[MAXPER], prevI[MAXPER];
+  int wake[MAXPER];
+#pragma unroll
+  for (int e = 0; e < MAXPER; ++e) {
+    const int i = min(i0 + e, NI - 1);
+    const long long c = rowBase + i;
+    dv[e] = D[c];
+    sv[e] = cS[c];
+    ev[e] = cE[c];
+    nv[e] = cN[c];
+    wv[e] = cW[c];
+    bv[e] = b[c];
+    oldI[e] = oldRow[i];
+    oldE[e] = oldRow[min(i + 1, NI - 1)];
+    northI[e] = hasNorth ? northRow[i] : T(0);
+    prevI[e] = (j > 0) ? rowPrev[i] : T(0);
+    wake[e] = (j == 0) ? I.acrossJ0[i] : -1;
+  }
+  const int segments = (j == 0) ? 2 : 1;
+  T carry = T(0);
+  for (int seg = 0; seg < segments; ++seg) {
+    const int lo = (segments == 1) ? 0 : (seg == 0 ? 0 : NI / 2);
+    const int hi = (segments == 1) ? NI : (seg == 0 ? NI / 2 : NI);
+    T pv[MAXPER], qv[MAXPER];
+    T P = T(0), Q = T(1);
+#pragma unroll
+    for (int e = 0; e < MAXPER; ++e) {
+      pv[e] = T(0);
+      qv[e] = T(1);
+      const int i = i0 + e;
+      if (e >= per || i < lo || i >= hi) continue;
+      const T d = dv[e];
+      if (!(fabs(d) > T(0))) {
+        pv[e] = oldI[e];
+        qv[e] = T(0);
+      } else {
+        T off = T(0);
+        if (j > 0) {
+          off += sv[e] * prevI[e];
+        } else {
+          const int a = wake[e];
+          if (a >= 0) off += sv[e] * ((a < i) ? rowNew[a] : oldRow[a]);
+        }
+        if (i < NI - 1) off += ev[e] * oldE[e];
+        if (hasNorth) off += nv[e] * northI[e];
+        pv[e] = (bv[e] - off) / d;
+        qv[e] = (i > 0) ? -wv[e] / d : T(0);
+      }
+      P = pv[e] + qv[e] * P;
+      Q = qv[e] * Q;
+    }
+    blockAffineExclusiveScan(P, Q, sc);
+    T xv = P + Q * carry;  // value entering this thread's chunk
+#pragma unroll
+    for (int e = 0; e < MAXPER; ++e) {
+      const int i = i0 + e;
+      if (e >= per || i < lo || i >= hi) continue;
+      xv = pv[e] + qv[e] * xv;
+      rowNew[i] = xv;
+    }
+    __syncthreads();
+    if (hi > lo) carry = rowNew[hi - 1];
+  }
+}
+
+template <typename T>
+DEV void gsRowSolve(const Instance& I, int j, const SysView<T>& y, const T* oldRow, const T* northRow, T* rowNew,
+                    const T* rowPrev, T* sc) {
+  if (I.NI <= 2 * static_cast<int>(blockDim.x)) {
+    gsRowSolveN<T, 2>(I, j, y, oldRow, northRow, rowNew, rowPrev, sc);
+  } else {
+    gsRowSolveAny(I, j, y, oldRow, northRow, rowNew, rowPrev, sc);
+  }
+}
+
+/// One row of the sweep on the unknowns in place: solve from the unknowns,
+/// then publish row j to global memory (east/north reads of later rows and
+/// the next sweep) and to rowPrev (the south values of row j + 1). Every
+/// read of this row's old values and of rowPrev happened before the scan's
+/// barriers. Ends without a barrier (the caller synchronises before the
+/// next row).
+template <typename T>
+DEV void gsRow(const Instance& I, int j, const SysView<T>& y, T* rowNew, T* rowPrev, T* sc) {
+  T* x = y.x;
+  const int NI = I.NI;
+  gsRowSolve(I, j, y, x + static_cast<long long>(j) * NI, x + static_cast<long long>(j + 1) * NI, rowNew, rowPrev,
+             sc);
+  for (int i = threadIdx.x; i < NI; i += blockDim.x) {
     x[j * NI + i] = rowNew[i];
     rowPrev[i] = rowNew[i];
   }
@@ -652,6 +759,171 @@ DEV void gsRowScanPipelined(const Instance& I, Team& t, int sweeps, const SysVie
     if (active && j >= 0 && j < I.NJ) gsRow(I, j, y, rowNew, rowPrev, sc);
     if (active) prefetchRow(I, j + 1, y);  // the next step's row, over the barrier
     t.cl.sync();
+  }
+}
+
+// ---- the chained k/omega sweeps: rows pushed to the next stage ------------------
+
+constexpr int kChainSlots = 4;                    // ring rows per stage (Shared::chainBar)
+constexpr long long kChainSpinLimit = 1LL << 24;  // polls before a wait gives up (~0.3 s)
+
+/// Shared memory of gsRowScanChained, in elements of T.
+__host__ __device__ inline long long chainSmemElems(int NI) { return (2LL + kChainSlots) * NI + 64; }
+
+DEV unsigned smemAddr(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+/// The shared::cluster address of this CTA's shared-memory address `a` in CTA `rank`.
+DEV unsigned clusterAddr(unsigned a, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+DEV void mbarInit(unsigned long long* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(b)) : "memory");
+}
+/// This CTA's one arrival on the barrier's current phase, expecting `bytes`.
+DEV void mbarArm(unsigned long long* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(b)), "r"(bytes) : "memory");
+}
+/// Whether the phase of parity `parity` has completed (acquire, cluster scope).
+DEV bool mbarDone(const unsigned long long* b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smemAddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+/// Store v into another CTA's shared memory; its mbarrier counts the bytes.
+DEV void pushRemote(unsigned dst, double v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f64 [%0], %1, [%2];" ::"r"(dst), "d"(v),
+               "r"(bar)
+               : "memory");
+}
+DEV void pushRemote(unsigned dst, float v, unsigned bar) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];" ::"r"(dst), "f"(v),
+               "r"(bar)
+               : "memory");
+}
+DEV unsigned loadRelaxedCluster(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+DEV void storeRelaxedCluster(unsigned* p, unsigned v) {
+  asm volatile("st.relaxed.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+/// Kernel start: the ring barriers armed for the first kChainSlots rows (of
+/// `rowBytes` each), the release count at zero. Made visible to the peers and
+/// the async proxy before the kernel's first cluster barrier.
+DEV void chainSetup(Shared& sh, unsigned rowBytes) {
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kChainSlots; ++k) {
+      mbarInit(&sh.chainBar[k]);
+      mbarArm(&sh.chainBar[k], rowBytes);
+    }
+    sh.chainAck = 0u;
+    sh.chainNever = 0u;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+}
+
+/// The k and omega sweeps as a chain of 2 * sweeps CTAs, CTA (eq, s) running
+/// sweep s of equation eq (0: k, 1: omega), without cluster-wide barriers.
+/// Row g (counted over the launch: g = base + j, base = calls so far x NJ)
+/// travels through ring slot g % kChainSlots: as a stage finishes a row it
+/// pushes the values into the next stage's slot with st.async, whose bytes
+/// complete that slot's mbarrier; the next stage waits for rows j and j+1
+/// (its old own-row and north values), reads them from its own shared
+/// memory, and when done with row j re-arms the slot for row g + kChainSlots
+/// and writes g + 1 into its producer's release count, which the producer
+/// waits for before pushing into that slot again. The first stage reads the
+/// unknowns, the last writes them, so the values and the arithmetic are
+/// those of gsRowScanSweeps (the same bits). A wait that gives up sets
+/// kFaultChainWait in the launch's fault word and the call waits no more, so
+/// the launch always ends (and reports the fault). With `waitTest` the second
+/// stage also waits once per call for a count nothing sets, which gives up
+/// and reports the fault while the rows still flow as usual.
+template <typename T>
+DEV void gsRowScanChained(const Instance& I, Team& t, Shared& sh, int sweeps, const SysView<T>& kSys,
+                          const SysView<T>& wSys, T* smem, unsigned base, bool waitTest) {
+  const int role = static_cast<int>(t.rank);
+  if (role >= 2 * sweeps) return;
+  const int s = role % sweeps;
+  const bool hasProducer = s > 0, hasConsumer = s < sweeps - 1;
+  const SysView<T>& y = (role >= sweeps) ? wSys : kSys;
+  const int NI = I.NI, NJ = I.NJ;
+  const unsigned rowBytes = static_cast<unsigned>(NI * sizeof(T));
+  T* rowNew = smem;
+  T* rowPrev = smem + NI;
+  T* sc = smem + 2 * NI;
+  T* ring = smem + 2 * NI + 64;
+  const unsigned nextRing = hasConsumer ? clusterAddr(smemAddr(ring), role + 1) : 0u;
+  const unsigned nextBar = hasConsumer ? clusterAddr(smemAddr(&sh.chainBar[0]), role + 1) : 0u;
+  unsigned* producerAck = hasProducer ? t.cl.map_shared_rank(&sh.chainAck, role - 1) : nullptr;
+  T* x = y.x;
+  bool faulted = false;  // a wait of this call gave up: the call waits no more
+  prefetchRow(I, 0, y);
+  for (int j = 0; j < NJ; ++j) {
+    const unsigned g = base + static_cast<unsigned>(j);
+    const unsigned slot = g % kChainSlots, slotN = (g + 1) % kChainSlots;
+    if (threadIdx.x == 0 && waitTest && s == 1 && j == 0) {
+      // test: once per call the second stage waits for a count nothing sets
+      long long spins = 0;
+      while (loadRelaxedCluster(&sh.chainNever) == 0u && ++spins <= kChainSpinLimit) {
+      }
+      if (spins > kChainSpinLimit) atomicOr(I.iterations + 1, kFaultChainWait);
+    }
+    if (threadIdx.x == 0 && !faulted) {
+      long long spins = 0;
+      for (;;) {
+        bool ready = true;
+        if (hasProducer) {
+          ready = mbarDone(&sh.chainBar[slot], (g / kChainSlots) & 1u) &&
+                  (j + 1 >= NJ || mbarDone(&sh.chainBar[slotN], ((g + 1) / kChainSlots) & 1u));
+        }
+        // the next stage has released the row this slot held (g - kChainSlots)
+        if (ready && hasConsumer && g + 1 >= kChainSlots) {
+          ready = loadRelaxedCluster(&sh.chainAck) >= g + 1 - kChainSlots;
+        }
+        if (ready) break;
+        if (++spins > kChainSpinLimit) {
+          atomicOr(I.iterations + 1, kFaultChainWait);
+          faulted = true;
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    const long long row = static_cast<long long>(j) * NI;
+    const T* oldRow = hasProducer ? ring + slot * NI : x + row;
+    const T* northRow = hasProducer ? ring + slotN * NI : x + row + NI;
+    gsRowSolve(I, j, y, oldRow, northRow, rowNew, rowPrev, sc);
+    // every read of ring slot `slot` happened before gsRowSolve's barriers
+    if (threadIdx.x == 0 && hasProducer) {
+      mbarArm(&sh.chainBar[slot], rowBytes);  // for row g + kChainSlots
+      storeRelaxedCluster(producerAck, g + 1);
+    }
+    for (int i = threadIdx.x; i < NI; i += blockDim.x) {
+      const T v = rowNew[i];
+      rowPrev[i] = v;
+      if (hasConsumer) {
+        pushRemote(nextRing + (slot * NI + i) * static_cast<unsigned>(sizeof(T)), v, nextBar + slot * 8u);
+      } else {
+        x[row + i] = v;
+      }
+    }
+    prefetchRow(I, j + 1, y);
+    if (!hasProducer && j + 2 < NJ) {
+      // the first stage's next north row (the unknowns, fixed until the last stage writes them)
+      constexpr int perLine = 128 / static_cast<int>(sizeof(T));
+      for (int q = threadIdx.x; q * perLine < NI; q += blockDim.x) {
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(x + row + 2 * NI + q * perLine));
+      }
+    }
+    // the next row's wait ends in a barrier, which orders these rowPrev
+    // writes and rowNew reads before the next row's use of them
   }
 }
 
@@ -1647,6 +1919,9 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
   const bool cgInShared = !(flags & (kFlagGlobalCg | kFlagTwoReductionCg)) && I.NJ >= static_cast<int>(t.R) &&
                           cgSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
   const bool leader = (t.rank == 0 && t.tid == 0);
+  // Ordered before any peer's access by the first cluster barrier below.
+  chainSetup(sh, static_cast<unsigned>(I.NI) * ((I.precision == 1) ? 4u : 8u));
+  if (leader) I.iterations[1] = 0;
 
   int done = 0;
   const int limit = (I.iterLimit < iterations) ? I.iterLimit : iterations;
@@ -1789,13 +2064,18 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
       // k and omega sweep in the reference's cell order: their floors and
       // the wall-cell omega override act after the sweeps, so the converged
       // state depends on the order (a colouring would move it by ~1e-3).
+      const bool chained = t.R >= 6 && !(flags & (kFlagSequentialRows | kFlagBarrierSweeps));
+      const unsigned chainBase = static_cast<unsigned>(it) * static_cast<unsigned>(I.NJ);
+      const bool waitTest = (flags & kFlagChainWaitTest) != 0;
       if (!(flags & kFlagPlainWavefront) && I.NI <= 8 * t.T &&
           (2 * I.NI + 64) * 8 <= smemBytes) {
         if (I.precision == 1) {
           // mixed form: the same sweep map on the FP32 corrections
           float* fs = reinterpret_cast<float*>(dyn);
           const SysView<float> ks = correctionSystem(I.tk), ws = correctionSystem(I.tw);
-          if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
+          if (chained && chainSmemElems(I.NI) * 4 <= smemBytes) {
+            gsRowScanChained(I, t, sh, 3, ks, ws, fs, chainBase, waitTest);
+          } else if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
             gsRowScanPipelined(I, t, 3, ks, ws, fs);
           } else if (t.R == 1) {
             gsRowScanSweeps(I, 3, ks, fs);
@@ -1805,6 +2085,8 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
           } else if (t.rank == 1) {
             gsRowScanSweeps(I, 3, ws, fs);
           }
+        } else if (chained && chainSmemElems(I.NI) * 8 <= smemBytes) {
+          gsRowScanChained(I, t, sh, 3, kSystem(I), omegaSystem(I), dyn, chainBase, waitTest);
         } else if (t.R >= 6 && !(flags & kFlagSequentialRows)) {
           gsRowScanPipelined(I, t, 3, kSystem(I), omegaSystem(I), dyn);
         } else if (t.R == 1) {
@@ -1903,9 +2185,12 @@ int kernelFlags() {
   // CG in global memory, bit 1 uses the plain wavefront sweeps, bit 2 runs
   // the k/omega row sweeps one after another instead of pipelined across
   // CTAs, bit 4 runs the global-memory CG in one pass per iteration
-  // instead of two (these four give identical results); bit 3 runs the
-  // reference's two-reduction CG instead of the single-reduction one (the
-  // same to rounding).
+  // instead of two, bit 5 pipelines the k/omega row sweeps with a cluster
+  // barrier per row instead of chaining them through DSMEM (these five give
+  // identical results); bit 3 runs the reference's two-reduction CG instead
+  // of the single-reduction one (the same to rounding). Bit 6 is for tests:
+  // a chained k/omega stage also waits for a count that nothing sets, so
+  // that wait gives up and the launch reports its fault word.
   const char* env = std::getenv("CFD_KERNEL_FLAGS");
   return (env != nullptr) ? std::atoi(env) : 0;
 }

@@ -39,6 +39,12 @@ Status fail(Status code, const std::string& message) {
   return code;
 }
 
+Status launchFault(int word) {
+  std::string what = "the solver kernel stopped waiting";
+  if (word & kFaultChainWait) what += " (a k/omega sweep stage for its neighbour)";
+  return fail(CFD_INTERNAL, what + "; the launch's results are not valid");
+}
+
 // ---- settings -----------------------------------------------------------------
 
 Settings fromC(const cfd_settings& s) {
@@ -322,7 +328,7 @@ Status Solver::build(const cfd_mesh_desc& m, const cfd_face_bc& bc) {
     I.mfN = a.take<double>(FN); I.mfE = a.take<double>(FE);
     I.pN = a.take<double>(FN); I.pE = a.take<double>(FE);
     I.history = a.take<double>(static_cast<std::size_t>(historyCapacity_) * kMonSlots);
-    I.iterations = a.take<int>(1);
+    I.iterations = a.take<int>(2);  // iterations, then the launch's fault word
     dCentroids_ = a.take<double>(2 * N);
     dWallCentres_ = a.take<double>(std::max<std::size_t>(wallCentres.size(), 2));
     dView_ = a.take<Instance>(1);
@@ -507,6 +513,11 @@ void Solver::planMultigrid(const std::vector<int>& wake0) {
       if (pa >= 0 && pb >= 0 && pa != pb) ok = false;
       c.wake[I] = (pa >= 0) ? pa : pb;
       if (c.wake[I] == I) ok = false;
+      // The level's red-black sweeps update a colour's cells concurrently, so
+      // partners across the cut must have opposite colours (both in row 0:
+      // I + wake[I] odd); with an odd number of columns they would not, and
+      // the two cells would read each other while both are written.
+      if (c.wake[I] >= 0 && ((I + c.wake[I]) & 1) == 0) ok = false;
     }
     if (!ok) break;
     mgShape_.push_back(std::move(c));
@@ -802,8 +813,10 @@ Status Solver::iterate(int n, int stopStage, double tolerance, std::vector<doubl
       return st;
     }
     CUDA_OR_FAIL(cudaStreamSynchronize(stream_));
-    int ran = 0;
-    CUDA_OR_FAIL(cudaMemcpy(&ran, dIterations_, sizeof(int), cudaMemcpyDeviceToHost));
+    int words[2] = {0, 0};
+    CUDA_OR_FAIL(cudaMemcpy(words, dIterations_, sizeof(words), cudaMemcpyDeviceToHost));
+    if (words[1] != 0) return launchFault(words[1]);
+    const int ran = words[0];
     if (history != nullptr && ran > 0) {
       const std::size_t old = history->size();
       history->resize(old + static_cast<std::size_t>(ran) * kMonSlots);
@@ -1419,9 +1432,11 @@ cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last) {
   if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
   for (std::size_t k = 0; k < b->handles.size(); ++k) {
     const cfdb::Instance& I = b->handles[k]->solver->deviceView();
-    int ran = 0;
-    e = cudaMemcpy(&ran, I.iterations, sizeof(int), cudaMemcpyDeviceToHost);
+    int words[2] = {0, 0};
+    e = cudaMemcpy(words, I.iterations, sizeof(words), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    if (words[1] != 0) return cfdb::launchFault(words[1]);
+    const int ran = words[0];
     if (taken != nullptr) taken[k] = ran;
     if (last != nullptr && ran > 0) {
       double h[cfdb::kMonSlots];

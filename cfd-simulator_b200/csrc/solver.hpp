@@ -217,6 +217,11 @@ Status launchSimple(const Instance* dInstances, int count, int clusterSize, int 
                     int iterations, int stopStage, double tolerance, cudaStream_t stream,
                     int smemBytes);
 
+/// The error for a launch whose fault word (Instance::iterations[1]) is
+/// nonzero: a bounded wait inside the kernel gave up, so its results are not
+/// to be used.
+Status launchFault(int word);
+
 /// Dynamic shared memory the pressure CG needs to keep a solve's band on
 /// chip (0: it does not fit and the CG runs from global memory).
 int cgSharedBytes(int NI, int NJ, int clusterSize);

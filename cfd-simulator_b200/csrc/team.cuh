@@ -27,6 +27,13 @@ struct Shared {
   double warp[kMaxWarps][kRedSlots];
   double part[2][kRedSlots];
   double result[kRedSlots];
+  // the chained k/omega sweeps: one mbarrier per ring slot, completed by the
+  // bytes of a row the previous stage pushes (st.async), and the count of
+  // rows the next stage has released, written by it through DSMEM; set up
+  // at kernel start
+  unsigned long long chainBar[4];
+  unsigned chainAck;
+  unsigned chainNever;  // stays 0: the wait test's condition
 };
 
 struct Team {

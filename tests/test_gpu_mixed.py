@@ -122,3 +122,28 @@ def test_precision_is_fixed_at_create():
     d = c.device(precision=1)
     with pytest.raises(cb.CfdError):
         d.set_settings(c.settings(precision=0))
+
+
+@pytest.mark.parametrize("ctas", [8, 16])
+def test_mixed_form_gives_the_same_bits_every_run(ctas, monkeypatch):
+    # A C-grid 70 cells around: halving it gives 35 columns, where cells
+    # across the wake cut would share a red-black colour, so the multigrid
+    # stops coarsening before that level (two partners updated in the same
+    # half-sweep would read each other, and the bits would vary from run to
+    # run). On 8 and 16 CTAs (most of them owning one row or none), repeated
+    # solves, in one launch or in launches of one iteration, agree bit for bit.
+    monkeypatch.setenv("CFD_CLUSTER_SIZE", str(ctas))
+    mesh = cb.cgrid("0012", surface_points=24, wake_points=12, normal_points=13, first_layer_height=1e-4,
+                    upstream_chords=10.0, downstream_chords=15.0, vertical_chords=10.0)
+    settings = cb.Settings.defaults(inflow_viscosity_ratio=10.0, precision=1)
+    runs = []
+    for chunk in (100, 100, 100, 1):
+        s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0), settings)
+        s.set_turbulence_model(cb.MODEL_SST)
+        s.initialise(*cb.uniform_field(mesh, 1.0, 4.0, 1.0, 1e6))
+        for _ in range(100 // chunk):
+            s.iterate(chunk)
+        runs.append(np.concatenate([s.read(f) for f in ("U", "V", "P", "K", "OMEGA")]))
+        s.close()
+    for r in runs[1:]:
+        assert np.array_equal(r, runs[0])

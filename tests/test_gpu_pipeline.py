@@ -1,7 +1,8 @@
 """Launch shapes and kernel implementation choices change where the work runs,
-not the arithmetic: the k/omega sweeps pipelined across CTAs give the same
-bits as the same sweeps one after another, and a solve on a wide cluster
-tracks the oracle as closely as on one CTA."""
+not the arithmetic: the k/omega sweeps chained across CTAs through DSMEM,
+or pipelined with a cluster barrier per row, give the same bits as the same
+sweeps one after another, and a solve on a wide cluster tracks the oracle as
+closely as on one CTA."""
 import os
 
 import numpy as np
@@ -32,27 +33,44 @@ class _env:
                 os.environ[k] = v
 
 
-def _medium_sst(iterations, flags):
+def _medium_sst(iterations, flags, precision=0):
     mesh = cb.cgrid("0012", surface_points=128, wake_points=65, normal_points=97,
                     first_layer_height=1e-5, upstream_chords=10.0, downstream_chords=15.0,
                     vertical_chords=10.0)
     with _env(CFD_KERNEL_FLAGS=flags):
         s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, 4.0),
-                                   cb.Settings.defaults(inflow_viscosity_ratio=10.0))
+                                   cb.Settings.defaults(inflow_viscosity_ratio=10.0, precision=precision))
         s.set_turbulence_model(cb.MODEL_SST)
         s.initialise(*cb.uniform_field(mesh, 1.0, 4.0, 1.0, 1e6))
         _, hist = s.iterate(iterations, history=True)
     return {f: s.read(f) for f in FIELDS}, hist
 
 
-def test_pipelined_sweeps_are_bit_identical_to_sequential_rows():
-    # 384 x 96 cells: a 16-CTA cluster, so the k/omega sweeps run pipelined
-    # over six CTAs by default and row after row with flag bit 2.
-    a, ha = _medium_sst(6, 0)
-    b, hb = _medium_sst(6, 4)
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("flags", [32, 4])
+def test_chained_sweeps_are_bit_identical_to_the_other_forms(flags, precision):
+    # 384 x 96 cells: a 16-CTA cluster, so the k/omega sweeps run chained
+    # over six CTAs by default, pipelined with a cluster barrier per row with
+    # flag bit 5 and row after row on two CTAs with flag bit 2 (in the mixed
+    # form the same three, on the FP32 corrections).
+    a, ha = _medium_sst(6, 0, precision)
+    b, hb = _medium_sst(6, flags, precision)
     assert np.array_equal(ha, hb)
     for f in FIELDS:
         assert np.array_equal(a[f], b[f]), f
+
+
+def test_a_chain_wait_that_gives_up_is_reported_and_the_device_stays_usable():
+    # flag bit 6 makes the second chained k/omega stage also wait for a count
+    # that nothing sets: that wait gives up after its poll limit, the launch
+    # finishes, and the host reads the fault word as an error.
+    with pytest.raises(cb.CfdError) as err:
+        _medium_sst(1, 64)
+    assert err.value.code == 8  # CFD_INTERNAL
+    assert "k/omega sweep stage" in str(err.value)
+    a, ha = _medium_sst(2, 0)
+    b, hb = _medium_sst(2, 32)
+    assert np.all(np.isfinite(ha)) and np.array_equal(ha, hb)
 
 
 def test_shared_and_global_memory_cg_are_bit_identical():
