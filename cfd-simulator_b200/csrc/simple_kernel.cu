@@ -361,38 +361,72 @@ DEV void gsColourMixed(const Instance& I, Team& t, int colour, bool last) {
   }
 }
 
-/// One red-black Gauss-Seidel colour pass on one or two systems sharing the
-/// cell order (LinearSystem.cpp:77-116, off-diagonals summed S, E, N, W).
-DEV void gsColour(const Instance& I, Team& t, int colour, const double* D, const double* cS,
-                  const double* cN, const double* cW, const double* cE, const double* b1, double* x1,
-                  const double* D2, const double* cS2, const double* cN2, const double* cW2,
-                  const double* cE2, const double* b2, double* x2) {
-  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-    const int i = c % I.NI, j = c / I.NI;
-    if (((i + j) & 1) != colour) continue;
-    const int nS = across(I, c, i, j, 0), nN = across(I, c, i, j, 1);
-    const int nW = across(I, c, i, j, 2), nE = across(I, c, i, j, 3);
-    {
-      const double d = D[c];
-      if (fabs(d) > 0.0) {
-        double off = 0.0;
-        if (nS >= 0) off += cS[c] * x1[nS];
-        if (nE >= 0) off += cE[c] * x1[nE];
-        if (nN >= 0) off += cN[c] * x1[nN];
-        if (nW >= 0) off += cW[c] * x1[nW];
-        x1[c] = (b1[c] - off) / d;
+/// One colour of a red-black Gauss-Seidel sweep of the momentum system for u
+/// and v together (one matrix, two right-hand sides; LinearSystem.cpp:77-116
+/// per cell, off-diagonals summed S, E, N, W). Threads take only the cells of
+/// the colour (a row holds ceil(NI/2) slots; i = 2k + ((j + colour) & 1)),
+/// two at a time, and issue every load of both cells before the arithmetic:
+/// a missing neighbour's index is clamped to the cell itself and its term is
+/// left out exactly as before, so the sums and the bits are unchanged.
+DEV void gsColour(const Instance& I, Team& t, int colour) {
+  const double* __restrict__ D = I.aD;
+  const double* __restrict__ cS = I.aS;
+  const double* __restrict__ cN = I.aN;
+  const double* __restrict__ cW = I.aW;
+  const double* __restrict__ cE = I.aE;
+  const double* __restrict__ bu = I.bU;
+  const double* __restrict__ bv = I.bV;
+  double* __restrict__ u = I.u;
+  double* __restrict__ v = I.v;
+  const int NI = I.NI;
+  const int H = (NI + 1) / 2;
+  const int j0 = t.c0 / NI;
+  const int slots = ((t.c1 - t.c0) / NI) * H;
+  constexpr int kPair = 2;
+  for (int q0 = t.tid; q0 < slots; q0 += kPair * t.T) {
+    int cell[kPair], nb[kPair][4];
+    bool ok[kPair];
+    double d[kPair], a[kPair][4], b1[kPair], b2[kPair], x1[kPair][4], x2[kPair][4];
+#pragma unroll
+    for (int e = 0; e < kPair; ++e) {
+      const int q = min(q0 + e * t.T, slots - 1);
+      const int j = j0 + q / H;
+      const int i = 2 * (q % H) + ((j + colour) & 1);
+      ok[e] = (q0 + e * t.T < slots) && i < NI;
+      const int ic = min(i, NI - 1);
+      const int c = j * NI + ic;
+      cell[e] = c;
+      nb[e][0] = across(I, c, ic, j, 0);  // S
+      nb[e][1] = across(I, c, ic, j, 3);  // E
+      nb[e][2] = across(I, c, ic, j, 1);  // N
+      nb[e][3] = across(I, c, ic, j, 2);  // W
+      d[e] = D[c];
+      a[e][0] = cS[c];
+      a[e][1] = cE[c];
+      a[e][2] = cN[c];
+      a[e][3] = cW[c];
+      b1[e] = bu[c];
+      b2[e] = bv[c];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int n = (nb[e][k] >= 0) ? nb[e][k] : c;
+        x1[e][k] = u[n];
+        x2[e][k] = v[n];
       }
     }
-    if (x2 != nullptr) {
-      const double d = D2[c];
-      if (fabs(d) > 0.0) {
-        double off = 0.0;
-        if (nS >= 0) off += cS2[c] * x2[nS];
-        if (nE >= 0) off += cE2[c] * x2[nE];
-        if (nN >= 0) off += cN2[c] * x2[nN];
-        if (nW >= 0) off += cW2[c] * x2[nW];
-        x2[c] = (b2[c] - off) / d;
+#pragma unroll
+    for (int e = 0; e < kPair; ++e) {
+      if (!ok[e] || !(fabs(d[e]) > 0.0)) continue;
+      double o1 = 0.0, o2 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (nb[e][k] >= 0) {
+          o1 += a[e][k] * x1[e][k];
+          o2 += a[e][k] * x2[e][k];
+        }
       }
+      u[cell[e]] = (b1[e] - o1) / d[e];
+      v[cell[e]] = (b2[e] - o2) / d[e];
     }
   }
 }
@@ -1964,8 +1998,7 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
     }
     for (int sweep = 0; sweep < I.sweeps && I.precision == 0; ++sweep) {
       for (int colour = 0; colour < 2; ++colour) {
-        gsColour(I, t, colour, I.aD, I.aS, I.aN, I.aW, I.aE, I.bU, I.u, I.aD, I.aS, I.aN, I.aW,
-                 I.aE, I.bV, I.v);
+        gsColour(I, t, colour);
         t.cl.sync();
       }
     }
