@@ -1701,12 +1701,16 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
   const int c0 = t.c0;
   // cells of this thread in the band: c0 + tid + k T, k < own
   const int own = (t.c1 - t.c0 > t.tid) ? (t.c1 - t.c0 - t.tid + t.T - 1) / t.T : 0;
+  // (i, j) of this thread's first cell and of the band's last, and the step
+  // between a thread's consecutive cells
+  const int firstI = (t.c0 + t.tid) % NI, firstJ = (t.c0 + t.tid) / NI;
+  const int lastI = (t.c1 - 1) % NI, lastJ = (t.c1 - 1) / NI;
+  const int stepI = t.T % NI, stepJ = t.T / NI;
   const double* below = (rank > 0) ? t.cl.map_shared_rank(ex, rank - 1) : nullptr;
   const double* above = (rank < R - 1) ? t.cl.map_shared_rank(ex, rank + 1) : nullptr;
   auto slot = [NI](int parity, int row, int value) { return ((parity * 2 + row) * 3 + value) * NI; };
   const int j0 = t.c0 / NI, j1 = t.c1 / NI;
-  auto exportRows = [&](int parity, int c, double r, double w, double s) {
-    const int i = c % NI, j = c / NI;
+  auto exportRows = [&](int parity, int i, int j, double r, double w, double s) {
     if (j == j0) {
       ex[slot(parity, 0, 0) + i] = r;
       ex[slot(parity, 0, 1) + i] = w;
@@ -1735,7 +1739,8 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
     wv[c] = y;
     pv[c] = 0.0;
     sv[c] = 0.0;
-    exportRows(0, c, rv[c], y, 0.0);
+    ub[c - c0] = un;  // u0: pass 1 of the first iteration takes M^-1 r from here
+    exportRows(0, i, j, rv[c], y, 0.0);
   }
   teamReduce(t, sh, acc, op1);
   if (!(fabs(acc[0]) > 0.0)) return 0;
@@ -1791,7 +1796,9 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
           const int c = t.c0 + t.tid + (k + u) * t.T;
           const double dg = cD[u];
           const double rc0 = cR[u];
-          const double pc = precondition(rc0, dg) + beta * cP[u];
+          // M^-1 r of the previous iteration: the u this thread stored for
+          // the cell then (the same operation on the same r, so the same bits)
+          const double pc = ub[c - c0] + beta * cP[u];
           const double sc = cW[u] + beta * cS[u];
           xv[c] = cX[u] + alpha * pc;
           const double rc = rc0 - alpha * sc;
@@ -1810,26 +1817,40 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
     // neighbours; the coefficient loads pipelined as in pass 1 (every face
     // index is in range for any cell, so they are loaded unconditionally).
     {
+      // the cell of the next load as (i, j), stepped by T cells per load
+      // (no integer division per cell); past the band, loads repeat its
+      // last cell and their values are not used
+      int li = firstI, lj = firstJ;
       double nD[kCgPair], nNs[kCgPair], nNn[kCgPair], nEw[kCgPair], nEe[kCgPair];
-      int nWk[kCgPair];
-      auto load = [&](int k, int u) {
-        const int c = min(t.c0 + t.tid + k * t.T, t.c1 - 1);
-        const int i = c % NI, j = c / NI;
+      int nI[kCgPair], nJ[kCgPair], nWk[kCgPair];
+      auto load = [&](int kk, int u) {
+        const bool in = kk < own;
+        const int i = in ? li : lastI, j = in ? lj : lastJ;
+        const int c = j * NI + i;
+        nI[u] = i;
+        nJ[u] = j;
         nD[u] = pD[c];
-        nNs[u] = pN[j * NI + i];
-        nNn[u] = pN[(j + 1) * NI + i];
-        nEw[u] = pE[j * (NI + 1) + i];
-        nEe[u] = pE[j * (NI + 1) + i + 1];
-        nWk[u] = wake[i];
+        nNs[u] = pN[c];           // face (i, j): south
+        nNn[u] = pN[c + NI];      // face (i, j + 1): north
+        nEw[u] = pE[c + j];       // face j (NI + 1) + i: west
+        nEe[u] = pE[c + j + 1];   // east
+        nWk[u] = (j == 0) ? wake[i] : -1;
+        li += stepI;
+        lj += stepJ;
+        if (li >= NI) {
+          li -= NI;
+          lj += 1;
+        }
       };
 #pragma unroll
       for (int u = 0; u < kCgPair; ++u) load(u, u);
       for (int k = 0; k < own; k += kCgPair) {
         double cD[kCgPair], cNs[kCgPair], cNn[kCgPair], cEw[kCgPair], cEe[kCgPair];
-        int cWk[kCgPair];
+        int cI[kCgPair], cJ[kCgPair], cWk[kCgPair];
 #pragma unroll
         for (int u = 0; u < kCgPair; ++u) {
-          cD[u] = nD[u]; cNs[u] = nNs[u]; cNn[u] = nNn[u]; cEw[u] = nEw[u]; cEe[u] = nEe[u]; cWk[u] = nWk[u];
+          cD[u] = nD[u]; cNs[u] = nNs[u]; cNn[u] = nNn[u]; cEw[u] = nEw[u]; cEe[u] = nEe[u];
+          cI[u] = nI[u]; cJ[u] = nJ[u]; cWk[u] = nWk[u];
         }
         if (k + kCgPair < own) {
 #pragma unroll
@@ -1838,8 +1859,8 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
 #pragma unroll
         for (int u = 0; u < kCgPair; ++u) {
           if (k + u >= own) break;
-          const int c = t.c0 + t.tid + (k + u) * t.T;
-          const int i = c % NI, j = c / NI;
+          const int i = cI[u], j = cJ[u];
+          const int c = j * NI + i;
           const int m = c - c0;
           const double un = ub[m];
           double y = cD[u] * un;
@@ -1850,7 +1871,7 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
           if (i < NI - 1) y += cEe[u] * ub[m + 1];
           wv[c] = y;
           sums[1] += y * un;
-          if (j == j0 || j == j1 - 1) exportRows(par ^ 1, c, rv[c], y, sv[c]);
+          if (j == j0 || j == j1 - 1) exportRows(par ^ 1, i, j, rv[c], y, sv[c]);
         }
       }
     }
