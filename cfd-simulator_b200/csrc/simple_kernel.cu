@@ -1657,13 +1657,17 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
   return iterations;
 }
 
-/// Shared memory of cgGlobalSplit, in doubles: each CTA's boundary rows'
-/// r, w and s for the neighbouring CTAs (two parities x two rows x three
-/// values x NI), the next u of the two rows bordering its band (2 x NI), and
-/// the next u of its own band (the largest band's cells).
 /// Cells per software-pipeline group in cgGlobalSplit's passes.
 constexpr int kCgPair = 2;
 
+/// Shared memory of cgGlobalSplit, in doubles: each CTA's boundary rows'
+/// r, w and s for the neighbouring CTAs (two parities x two rows x three
+/// values x NI), the next u of the two rows bordering its band (2 x NI), and
+/// the next u of its own band (the largest band's cells). At 768x192 on 16
+/// CTAs this is 159.75 KB, which with the static shared memory stays within
+/// the SM's 164 KB shared-memory carve-out; any more moves the carve-out to
+/// 196 KB, shrinks the L1 cache by a third, and measured slower in every
+/// phase (halo diagonals held here: batched polar step 23.1 -> 23.5 ms).
 __host__ __device__ inline long long cgSplitSmemDoubles(int NI, int NJ, int R) {
   return 14LL * NI + cgSmemStride(NI, NJ, R);
 }
