@@ -51,12 +51,13 @@ enum Stage : int {
 };
 
 // Kernel implementation flags (bit mask).
-constexpr int kFlagGlobalCg = 1;
+constexpr int kFlagGlobalCg = 1;    // the default now; kept so the flag value stays accepted
 constexpr int kFlagPlainWavefront = 2;
 constexpr int kFlagSequentialRows = 4;
 constexpr int kFlagTwoReductionCg = 8;
 constexpr int kFlagOnePassCg = 16;
 constexpr int kFlagBarrierSweeps = 32;
+constexpr int kFlagSharedCg = 128;  // the pressure CG's band in shared memory where it fits
 constexpr int kFlagChainWaitTest = 64;  // tests only: a chained stage also waits for a count nothing sets
 
 // Fault codes a launch leaves in iterations[1] (bits, or-ed together).

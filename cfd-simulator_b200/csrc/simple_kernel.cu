@@ -1973,9 +1973,14 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
   t.c0 = I.NI * ((I.NJ * static_cast<int>(t.rank)) / static_cast<int>(t.R));
   t.c1 = I.NI * ((I.NJ * (static_cast<int>(t.rank) + 1)) / static_cast<int>(t.R));
   const bool sst = (I.model == 2);
-  // The pressure CG keeps its band in shared memory when every band has a
-  // row and the largest band's arrays fit in what the launch provides.
-  const bool cgInShared = !(flags & (kFlagGlobalCg | kFlagTwoReductionCg)) && I.NJ >= static_cast<int>(t.R) &&
+  // With kernel flag bit 7 the pressure CG keeps its band in shared memory
+  // when every band has a row and the largest band's arrays fit in what the
+  // launch provides. By default it runs from global memory in two passes
+  // (cgGlobalSplit), which measured faster on every benchmark grid (384x96
+  // on 16 CTAs: 1.98 against 2.54 ms per iteration; 192x48: 1.08 against
+  // 1.28 ms) and leaves most of the SM's shared memory to the L1 cache.
+  const bool cgInShared = (flags & kFlagSharedCg) && !(flags & kFlagTwoReductionCg) &&
+                          I.NJ >= static_cast<int>(t.R) &&
                           cgSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
   const bool leader = (t.rank == 0 && t.tid == 0);
   // Ordered before any peer's access by the first cluster barrier below.
@@ -2239,8 +2244,9 @@ int chooseClusterSize(int cells) {
 }
 
 int kernelFlags() {
-  // Implementation choices for tuning comparisons: bit 0 keeps the pressure
-  // CG in global memory, bit 1 uses the plain wavefront sweeps, bit 2 runs
+  // Implementation choices for tuning comparisons: bit 7 keeps the pressure
+  // CG's band in shared memory where it fits (bit 0, global memory, is the
+  // default now), bit 1 uses the plain wavefront sweeps, bit 2 runs
   // the k/omega row sweeps one after another instead of pipelined across
   // CTAs, bit 4 runs the global-memory CG in one pass per iteration
   // instead of two, bit 5 pipelines the k/omega row sweeps with a cluster
@@ -2253,13 +2259,16 @@ int kernelFlags() {
   return (env != nullptr) ? std::atoi(env) : 0;
 }
 
+int chainSweepBytes(int NI, int elemBytes) { return static_cast<int>(chainSmemElems(NI) * elemBytes); }
+
 int cgSharedBytes(int NI, int NJ, int clusterSize) {
-  // The k/omega row sweeps keep two rows and the scan's warp totals; the
-  // pressure CG its band (cgShared) or, where that does not fit, the
-  // exported boundary rows of the two-pass global-memory form.
-  const long long wave = (2LL * NI + 64) * 8;
+  // The chained k/omega row sweeps keep two rows, the scan's warp totals and
+  // a ring of rows; the pressure CG the exported boundary rows and the
+  // band's u of the two-pass global-memory form, or with kernel flag bit 7
+  // its whole band (cgShared) where that fits.
+  const long long wave = chainSmemElems(NI) * 8;
   long long bytes = 0;
-  if (NJ >= clusterSize) bytes = cgSmemDoubles(NI, NJ, clusterSize) * 8;
+  if (NJ >= clusterSize && (kernelFlags() & kFlagSharedCg)) bytes = cgSmemDoubles(NI, NJ, clusterSize) * 8;
   if (bytes > kMaxCgSharedBytes) bytes = 0;
   if (bytes == 0 && NJ >= clusterSize && cgSplitSmemDoubles(NI, NJ, clusterSize) * 8 <= kMaxCgSharedBytes) {
     bytes = cgSplitSmemDoubles(NI, NJ, clusterSize) * 8;

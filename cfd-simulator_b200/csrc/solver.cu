@@ -551,7 +551,7 @@ Status Solver::setLaunchShape(int clusterSize, int threads) {
 
 int Solver::launchSmemBytes(int clusterSize) const {
   if (settings_.precision == 1) {
-    const int scan = (2 * NI_ + 64) * 8;  // the k/omega row sweeps
+    const int scan = chainSweepBytes(NI_, 4);  // the chained k/omega row sweeps, FP32
     return std::max(mgSmemBytes_, (scan <= kMaxCgSharedBytes) ? scan : 0);
   }
   return cgSharedBytes(NI_, NJ_, clusterSize);

@@ -222,6 +222,10 @@ Status launchSimple(const Instance* dInstances, int count, int clusterSize, int 
 /// to be used.
 Status launchFault(int word);
 
+/// Dynamic shared memory of the chained k/omega sweeps on rows of NI cells
+/// of `elemBytes` each (two rows, the scan's warp totals and the ring).
+int chainSweepBytes(int NI, int elemBytes);
+
 /// Dynamic shared memory the pressure CG needs to keep a solve's band on
 /// chip (0: it does not fit and the CG runs from global memory).
 int cgSharedBytes(int NI, int NJ, int clusterSize);

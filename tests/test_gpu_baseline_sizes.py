@@ -4,8 +4,9 @@ single-solve benchmark configurations and of the batched polar.
 
 These sizes take launch paths the small golden cases never reach: clusters
 of 8 and 16 CTAs with DSMEM halos between row bands, the k/omega sweeps
-pipelined over six CTAs, the pressure CG from global memory (768x192, or any
-size with CFD_KERNEL_FLAGS=1; the reference's two-reduction CG with 8) and,
+chained over six CTAs, the pressure CG from global memory in two passes
+(its band in shared memory with CFD_KERNEL_FLAGS=128 where it fits; the
+reference's two-reduction CG with 8) and,
 in the mixed form, multigrid levels split over the cluster in global memory.
 Each is compared with the CPU oracle, which test_oracle_baseline_sizes.py
 pins bit for bit to the reference at the same sizes; the c1 solve also with
@@ -33,10 +34,10 @@ PRE_CG = [("GRADIENTS", ["GRAD_U", "GRAD_V", "GRAD_P"]),
           ("MOMENTUM_SOLVE", ["U", "V"]),
           ("RHIE_CHOW", ["MASS_FLUX"]),
           ("PRESSURE_ASSEMBLY", ["P_DIAG", "P_SOURCE", "P_UPPER", "NET_FLUX"])]
-# kernel flag bit 0: the pressure CG runs from global memory even where its
-# band fits in shared memory; bit 3: the reference's two-reduction CG instead
+# kernel flag bit 7: the pressure CG keeps its band in shared memory where it
+# fits (192x48 and 384x96); bit 3: the reference's two-reduction CG instead
 # of the single-reduction one. All must track the oracle alike.
-KERNEL_FLAGS = [0, 1, 8]
+KERNEL_FLAGS = [0, 128, 8]
 _CASES: dict = {}
 _TWENTY: dict = {}
 
