@@ -62,6 +62,7 @@ constexpr int kFlagChainWaitTest = 64;  // tests only: a chained stage also wait
 
 // Fault codes a launch leaves in iterations[1] (bits, or-ed together).
 constexpr int kFaultChainWait = 1;  // a chained k/omega sweep stage gave up waiting for its neighbour
+constexpr int kFaultHaloWait = 2;   // the pressure CG gave up waiting for a neighbour's halo row
 
 // Layout of one monitor record (cfd_monitor), in doubles.
 enum MonitorSlot : int {

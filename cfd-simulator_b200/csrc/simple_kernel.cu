@@ -849,10 +849,16 @@ DEV void storeRelaxedCluster(unsigned* p, unsigned v) {
 }
 
 /// Kernel start: the ring barriers armed for the first kChainSlots rows (of
-/// `rowBytes` each), the release count at zero. Made visible to the peers and
+/// `rowBytes` each), the release count at zero, and the split CG's halo
+/// barrier armed for the bytes the neighbouring CTAs push each iteration. Made visible to the peers and
 /// the async proxy before the kernel's first cluster barrier.
-DEV void chainSetup(Shared& sh, unsigned rowBytes) {
+DEV void chainSetup(Shared& sh, unsigned rowBytes, unsigned haloBytes) {
   if (threadIdx.x == 0) {
+    // cgGlobalSplit's halo barrier, armed for its first iteration
+    mbarInit(&sh.haloBar);
+    mbarArm(&sh.haloBar, haloBytes);
+    sh.haloPhase = 0u;
+    sh.haloBytes = haloBytes;
     for (int k = 0; k < kChainSlots; ++k) {
       mbarInit(&sh.chainBar[k]);
       mbarArm(&sh.chainBar[k], rowBytes);
@@ -1660,31 +1666,31 @@ DEV int cgGlobal(const Instance& I, Team& t, Shared& sh, double initial, double 
 /// Cells per software-pipeline group in cgGlobalSplit's passes.
 constexpr int kCgPair = 2;
 
-/// Shared memory of cgGlobalSplit, in doubles: each CTA's boundary rows'
-/// r, w and s for the neighbouring CTAs (two parities x two rows x three
-/// values x NI), the next u of the two rows bordering its band (2 x NI), and
-/// the next u of its own band (the largest band's cells). At 768x192 on 16
-/// CTAs this is 159.75 KB, which with the static shared memory stays within
-/// the SM's 164 KB shared-memory carve-out; any more moves the carve-out to
-/// 196 KB, shrinks the L1 cache by a third, and measured slower in every
-/// phase (halo diagonals held here: batched polar step 23.1 -> 23.5 ms).
+/// Shared memory of cgGlobalSplit, in doubles: the u of the two rows
+/// bordering the band, pushed there by the neighbouring CTAs (2 x NI), and
+/// the u of its own band (the largest band's cells). At 768x192 on 16 CTAs
+/// this is 84 KB, inside the SM's 100 KB shared-memory carve-out, which
+/// leaves the rest of the SM's 256 KB to the L1 cache: a larger carve-out
+/// measured slower in every phase.
 __host__ __device__ inline long long cgSplitSmemDoubles(int NI, int NJ, int R) {
-  return 14LL * NI + cgSmemStride(NI, NJ, R);
+  return 2LL * NI + cgSmemStride(NI, NJ, R);
 }
 
 /// The single-reduction PCG of cgGlobal in two passes per iteration, for
-/// bands in global memory, with r, w and s held once: the first pass forms
-/// each own cell's p, s, x, r and next u in place (u stored), and the next u
-/// of the two rows bordering the band from the r, w and s the neighbouring
-/// CTAs exported for them (u in shared memory); after a block barrier the
-/// second forms w' = A u' from them and exports the band's first and last
-/// rows' new r, w and s to this CTA's shared memory (double-buffered by
-/// iteration parity, read by the neighbours through DSMEM after the
-/// iteration's reduction). Each pass has few independent loads per cell, so
+/// bands in global memory, with r, w and s held once. The first pass forms
+/// each own cell's p, s, x, r and next u in place, keeps u in shared memory,
+/// and pushes the u of the band's first and last rows into the halo of the
+/// CTA below and above (st.async, completing that CTA's halo mbarrier); after
+/// waiting for its own halo rows and a block barrier, the second pass forms
+/// w' = A u'. A CTA's pushes for the next iteration follow the iteration's
+/// reduction, which the receiver reaches only after its second pass, so one
+/// halo buffer suffices. Each pass has few independent loads per cell, so
 /// they overlap across cells; the one-pass form's neighbour recomputation
 /// (four loads per neighbour, three vectors double-buffered) leaves it
 /// latency-bound and 30 % larger in L2. The same expressions in the same cell
-/// order as cgGlobal and cgShared, so the same bits.
+/// order as cgGlobal and cgShared, so the same bits. A halo wait that gives
+/// up sets kFaultHaloWait in the launch's fault word and the solve carries
+/// on without waiting again.
 DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double gamma) {
   const int NI = I.NI, NJ = I.NJ;
   const int R = static_cast<int>(t.R), rank = static_cast<int>(t.rank);
@@ -1697,11 +1703,10 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
   double* __restrict__ rv = I.r;
   double* __restrict__ wv = I.q;
   double* __restrict__ sv = I.d1;
-  // exports: [parity][row: 0 first, 1 last][value: r, w, s][i]; then the halo
-  // u and the band's own u (cell c at c - c0)
-  double* ex = dyn;
-  double* halo = dyn + 12 * NI;  // [0, NI): row j0 - 1; [NI, 2 NI): row j1
-  double* __restrict__ ub = dyn + 14 * NI;  // cell c at ub[c - c0]
+  // the u of the rows bordering the band, pushed here by the neighbouring
+  // CTAs ([0, NI): row j0 - 1; [NI, 2 NI): row j1), then the band's own u
+  double* halo = dyn;
+  double* __restrict__ ub = dyn + 2 * NI;  // cell c at ub[c - c0]
   const int c0 = t.c0;
   // cells of this thread in the band: c0 + tid + k T, k < own
   const int own = (t.c1 - t.c0 > t.tid) ? (t.c1 - t.c0 - t.tid + t.T - 1) / t.T : 0;
@@ -1710,22 +1715,17 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
   const int firstI = (t.c0 + t.tid) % NI, firstJ = (t.c0 + t.tid) / NI;
   const int lastI = (t.c1 - 1) % NI, lastJ = (t.c1 - 1) / NI;
   const int stepI = t.T % NI, stepJ = t.T / NI;
-  const double* below = (rank > 0) ? t.cl.map_shared_rank(ex, rank - 1) : nullptr;
-  const double* above = (rank < R - 1) ? t.cl.map_shared_rank(ex, rank + 1) : nullptr;
-  auto slot = [NI](int parity, int row, int value) { return ((parity * 2 + row) * 3 + value) * NI; };
   const int j0 = t.c0 / NI, j1 = t.c1 / NI;
-  auto exportRows = [&](int parity, int i, int j, double r, double w, double s) {
-    if (j == j0) {
-      ex[slot(parity, 0, 0) + i] = r;
-      ex[slot(parity, 0, 1) + i] = w;
-      ex[slot(parity, 0, 2) + i] = s;
-    }
-    if (j == j1 - 1) {
-      ex[slot(parity, 1, 0) + i] = r;
-      ex[slot(parity, 1, 1) + i] = w;
-      ex[slot(parity, 1, 2) + i] = s;
-    }
-  };
+  // where this band's first row goes (the halo's upper half in the CTA
+  // below) and its last row (the lower half in the CTA above), with their
+  // barriers; 0 where there is no neighbour
+  const bool hasBelow = rank > 0, hasAbove = rank < R - 1;
+  const unsigned toBelow = hasBelow ? clusterAddr(smemAddr(halo + NI), rank - 1) : 0u;
+  const unsigned toAbove = hasAbove ? clusterAddr(smemAddr(halo), rank + 1) : 0u;
+  const unsigned belowBar = hasBelow ? clusterAddr(smemAddr(&sh.haloBar), rank - 1) : 0u;
+  const unsigned aboveBar = hasAbove ? clusterAddr(smemAddr(&sh.haloBar), rank + 1) : 0u;
+  const int lastRow = t.c1 - NI;  // first cell of the band's last row
+  bool haloFaulted = false;
   // w0 = A u0 (u0 from b, stable since the start's reduction); p = s = 0
   double acc[1] = {0.0};
   const int op1[1] = {kSum};
@@ -1744,7 +1744,6 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
     pv[c] = 0.0;
     sv[c] = 0.0;
     ub[c - c0] = un;  // u0: pass 1 of the first iteration takes M^-1 r from here
-    exportRows(0, i, j, rv[c], y, 0.0);
   }
   teamReduce(t, sh, acc, op1);
   if (!(fabs(acc[0]) > 0.0)) return 0;
@@ -1754,23 +1753,8 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
   int iterations = 0;
   const int op3[3] = {kSum, kSum, kSum};
   for (int iter = 0; iter < I.cgMax; ++iter) {
-    const int par = iter & 1;
     const double alpha = k.alpha, beta = k.beta;
     double sums[3] = {0.0, 0.0, 0.0};
-    // the bordering rows' next u, from the r, w and s their CTAs exported
-    for (int q = t.tid; q < 2 * NI; q += t.T) {
-      const bool low = q < NI;
-      const double* src = low ? below : above;
-      if (src == nullptr) continue;
-      const int i = low ? q : q - NI;
-      const int row = low ? 1 : 0;  // the CTA below exports its last row, the one above its first
-      const double rn = src[slot(par, row, 0) + i];
-      const double wn = src[slot(par, row, 1) + i];
-      const double sn = src[slot(par, row, 2) + i];
-      const int n = (low ? (j0 - 1) : j1) * NI + i;
-      const double s2 = wn + beta * sn;
-      halo[q] = precondition(rn - alpha * s2, pD[n]);
-    }
     // pass 1: own cells. Software-pipelined by hand: the next pair of cells'
     // loads are issued before this pair's arithmetic (the division's slow
     // path otherwise keeps the compiler from hoisting them), so two pairs of
@@ -1811,15 +1795,33 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
           sv[c] = sc;
           rv[c] = rc;
           ub[c - c0] = un;
+          // the band's first and last rows are the neighbours' halo rows
+          if (hasBelow && c < c0 + NI) pushRemote(toBelow + 8u * static_cast<unsigned>(c - c0), un, belowBar);
+          if (hasAbove && c >= lastRow) pushRemote(toAbove + 8u * static_cast<unsigned>(c - lastRow), un, aboveBar);
           sums[0] += rc * un;
           sums[2] += fabs(rc);
         }
       }
     }
+    // the neighbours' rows of this iteration (pushed in their pass 1); then
+    // the barrier is armed for the next iteration's, before this CTA can
+    // reach the reduction after which the neighbours push them
+    if (threadIdx.x == 0) {
+      long long spins = 0;
+      while (!haloFaulted && !mbarDone(&sh.haloBar, sh.haloPhase & 1u)) {
+        if (++spins > kChainSpinLimit) {
+          atomicOr(I.iterations + 1, kFaultHaloWait);
+          haloFaulted = true;
+        }
+      }
+      if (!haloFaulted) {
+        sh.haloPhase += 1u;
+        mbarArm(&sh.haloBar, sh.haloBytes);
+      }
+    }
     __syncthreads();
-    // pass 2: w' = A u', and the boundary rows' new r, w and s for the
-    // neighbours; the coefficient loads pipelined as in pass 1 (every face
-    // index is in range for any cell, so they are loaded unconditionally).
+    // pass 2: w' = A u'; the coefficient loads pipelined as in pass 1 (every
+    // face index is in range for any cell, so they are loaded unconditionally).
     {
       // the cell of the next load as (i, j), stepped by T cells per load
       // (no integer division per cell); past the band, loads repeat its
@@ -1875,7 +1877,6 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
           if (i < NI - 1) y += cEe[u] * ub[m + 1];
           wv[c] = y;
           sums[1] += y * un;
-          if (j == j0 || j == j1 - 1) exportRows(par ^ 1, i, j, rv[c], y, sv[c]);
         }
       }
     }
@@ -1984,7 +1985,8 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
                           cgSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes;
   const bool leader = (t.rank == 0 && t.tid == 0);
   // Ordered before any peer's access by the first cluster barrier below.
-  chainSetup(sh, static_cast<unsigned>(I.NI) * ((I.precision == 1) ? 4u : 8u));
+  chainSetup(sh, static_cast<unsigned>(I.NI) * ((I.precision == 1) ? 4u : 8u),
+             static_cast<unsigned>(I.NI) * 8u * ((t.rank > 0 ? 1u : 0u) + (t.rank + 1 < t.R ? 1u : 0u)));
   if (leader) I.iterations[1] = 0;
 
   int done = 0;

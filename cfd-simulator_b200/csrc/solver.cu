@@ -42,6 +42,7 @@ Status fail(Status code, const std::string& message) {
 Status launchFault(int word) {
   std::string what = "the solver kernel stopped waiting";
   if (word & kFaultChainWait) what += " (a k/omega sweep stage for its neighbour)";
+  if (word & kFaultHaloWait) what += " (the pressure CG for a neighbour's halo row)";
   return fail(CFD_INTERNAL, what + "; the launch's results are not valid");
 }
 

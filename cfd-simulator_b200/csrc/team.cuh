@@ -34,6 +34,11 @@ struct Shared {
   unsigned long long chainBar[4];
   unsigned chainAck;
   unsigned chainNever;  // stays 0: the wait test's condition
+  // the split pressure CG: the barrier the neighbouring CTAs' halo rows
+  // complete each iteration, its phase count and the bytes it expects
+  unsigned long long haloBar;
+  unsigned haloPhase;
+  unsigned haloBytes;
 };
 
 struct Team {
