@@ -338,25 +338,75 @@ DEV void phaseMomentum(const Instance& I, Team& t, double& resU, double& resV, d
 /// or v during the sweeps.
 DEV void gsColourMixed(const Instance& I, Team& t, int colour, bool last) {
   const Rows32& m = I.mom;
-  for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
-    const int i = c % I.NI, j = c / I.NI;
-    if (((i + j) & 1) == colour) {
-      const float d = m.D[c];
-      if (d != 0.0f) {
-        const int nS = across(I, c, i, j, 0), nN = across(I, c, i, j, 1);
-        const int nW = across(I, c, i, j, 2), nE = across(I, c, i, j, 3);
-        float ou = 0.0f, ov = 0.0f;
-        if (nS >= 0) { ou += m.S[c] * m.x[nS]; ov += m.S[c] * I.momXv[nS]; }
-        if (nE >= 0) { ou += m.E[c] * m.x[nE]; ov += m.E[c] * I.momXv[nE]; }
-        if (nN >= 0) { ou += m.N[c] * m.x[nN]; ov += m.N[c] * I.momXv[nN]; }
-        if (nW >= 0) { ou += m.W[c] * m.x[nW]; ov += m.W[c] * I.momXv[nW]; }
-        m.x[c] = (m.r[c] - ou) / d;
-        I.momXv[c] = (I.momRv[c] - ov) / d;
+  const float* __restrict__ D = m.D;
+  const float* __restrict__ cS = m.S;
+  const float* __restrict__ cN = m.N;
+  const float* __restrict__ cW = m.W;
+  const float* __restrict__ cE = m.E;
+  const float* __restrict__ ru = m.r;
+  const float* __restrict__ rv = I.momRv;
+  float* __restrict__ xu = m.x;
+  float* __restrict__ xv = I.momXv;
+  const int NI = I.NI;
+  const int H = (NI + 1) / 2;
+  const int j0 = t.c0 / NI;
+  const int slots = ((t.c1 - t.c0) / NI) * H;
+  constexpr int kPair = 2;
+  // only the colour's cells (i = 2k + ((j + colour) & 1)), two at a time,
+  // every load first; missing neighbours are clamped to the cell and their
+  // terms left out as before, so the sums are unchanged
+  for (int q0 = t.tid; q0 < slots; q0 += kPair * t.T) {
+    int cell[kPair], nb[kPair][4];
+    bool ok[kPair];
+    float d[kPair], a[kPair][4], b1[kPair], b2[kPair], x1[kPair][4], x2[kPair][4];
+#pragma unroll
+    for (int e = 0; e < kPair; ++e) {
+      const int q = min(q0 + e * t.T, slots - 1);
+      const int j = j0 + q / H;
+      const int i = 2 * (q % H) + ((j + colour) & 1);
+      ok[e] = (q0 + e * t.T < slots) && i < NI;
+      const int ic = min(i, NI - 1);
+      const int c = j * NI + ic;
+      cell[e] = c;
+      nb[e][0] = across(I, c, ic, j, 0);  // S
+      nb[e][1] = across(I, c, ic, j, 3);  // E
+      nb[e][2] = across(I, c, ic, j, 1);  // N
+      nb[e][3] = across(I, c, ic, j, 2);  // W
+      d[e] = D[c];
+      a[e][0] = cS[c];
+      a[e][1] = cE[c];
+      a[e][2] = cN[c];
+      a[e][3] = cW[c];
+      b1[e] = ru[c];
+      b2[e] = rv[c];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int n = (nb[e][k] >= 0) ? nb[e][k] : c;
+        x1[e][k] = xu[n];
+        x2[e][k] = xv[n];
       }
     }
-    if (last) {
-      I.u[c] += static_cast<double>(m.x[c]);
-      I.v[c] += static_cast<double>(I.momXv[c]);
+#pragma unroll
+    for (int e = 0; e < kPair; ++e) {
+      if (!ok[e] || d[e] == 0.0f) continue;
+      float ou = 0.0f, ov = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (nb[e][k] >= 0) {
+          ou += a[e][k] * x1[e][k];
+          ov += a[e][k] * x2[e][k];
+        }
+      }
+      xu[cell[e]] = (b1[e] - ou) / d[e];
+      xv[cell[e]] = (b2[e] - ov) / d[e];
+    }
+  }
+  if (last) {
+    // the corrections of the whole band (this CTA wrote all of them) onto u, v
+    __syncthreads();
+    for (int c = t.c0 + t.tid; c < t.c1; c += t.T) {
+      I.u[c] += static_cast<double>(xu[c]);
+      I.v[c] += static_cast<double>(xv[c]);
     }
   }
 }
