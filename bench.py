@@ -169,30 +169,33 @@ def _cluster_env(cluster: int):
             os.environ["CFD_CLUSTER_SIZE"] = previous
 
 
+def plain_cluster(designation: str, level: str) -> int:
+    """CTAs per solve of the plain form's batched polar. The 21 NACA 2412
+    points take 16-CTA clusters: a B200 holds 7 of those at once, so they fill
+    exactly three waves. The NACA 0012 trio runs beside them on the SMs those
+    clusters leave free, in a launch of its own: 768x192 on 8 CTAs, the two
+    smaller grids on 4. (All 24 on 16 CTAs take a fourth wave for the one
+    768x192 0012 solve: 18.9 against 17.9 ms per step.)"""
+    if designation == "2412":
+        return 16
+    return 8 if level == "fine" else 4
+
+
 def polar_solvers(cb, precision: int = 0, cluster: int | None = None, count: int | None = None):
     """The 24 solves of the batched polar (or its first `count`, for a
     profiling capture of a smaller case), created on the device from the
     uniform start. `cluster` fixes the CTAs per solve (the library's
-    CFD_CLUSTER_SIZE knob), else each solve takes the library's default."""
+    CFD_CLUSTER_SIZE knob), else each solve takes `plain_cluster`'s."""
     settings = cb.Settings.defaults(inflow_intensity=INTENSITY, inflow_viscosity_ratio=VISCOSITY_RATIO,
                                     precision=precision)
-    previous = os.environ.get("CFD_CLUSTER_SIZE")
-    if cluster is not None:
-        os.environ["CFD_CLUSTER_SIZE"] = str(cluster)
     meshes, solvers = {}, []
-    try:
-        for des, alpha, re, level, fl in POLAR[:count]:
-            mesh = _mesh(cb, des, level, fl, meshes)
+    for des, alpha, re, level, fl in POLAR[:count]:
+        mesh = _mesh(cb, des, level, fl, meshes)
+        with _cluster_env(cluster if cluster is not None else plain_cluster(des, level)):
             s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha), settings)
-            s.set_turbulence_model(cb.MODEL_SST)
-            s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, re))
-            solvers.append(s)
-    finally:
-        if cluster is not None:
-            if previous is None:
-                os.environ.pop("CFD_CLUSTER_SIZE", None)
-            else:
-                os.environ["CFD_CLUSTER_SIZE"] = previous
+        s.set_turbulence_model(cb.MODEL_SST)
+        s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, re))
+        solvers.append(s)
     return solvers
 
 
@@ -513,7 +516,9 @@ def run_ours(args) -> None:
         config = c2_config() if c2 else polar_config({"solves": len(solvers), "cells": cells})
         if not c2 and args.solves is not None:
             config["workload"] += f" (only the first {len(solvers)} solves: a profiling case)"
-        config.update({"cluster_shape": shape, "launch": "cuda graph" if args.graph else "direct",
+        config.update({"cluster_shape": shape, "cluster_sizes": sorted(
+                           {plain_cluster(d, lv) for d, _, _, lv, _ in POLAR[:args.solves]}, reverse=True)
+                       if not (c2 or mixed_only) else [shape[0]], "launch": "cuda graph" if args.graph else "direct",
                        "cg_iterations_per_solve": cg})
         if mixed_only:
             config["precision"] = "mixed: FP64 assembly/state, FP32 sweeps and multigrid CG"

@@ -1321,13 +1321,24 @@ cfd_status cfd_gpu_destroy(cfd_handle h) {
 
 // ---- batches ------------------------------------------------------------------------------
 
+/// The solves of a batch that share a launch shape: one launch over a
+/// contiguous part of the descriptor table, on a stream of its own.
+struct BatchGroup {
+  int offset{0}, count{0};
+  int clusterSize{1}, threads{512}, smemBytes{0};
+  std::vector<int> members;  // indices into cfd_batch_t::handles
+  cudaStream_t stream{nullptr};
+  cudaEvent_t done{nullptr};
+};
+
 struct cfd_batch_t {
   std::vector<cfd_handle> handles;
   cfdb::Instance* dTable{nullptr};
   cudaStream_t stream{nullptr};
-  int clusterSize{1};
+  cudaEvent_t fork{nullptr};
+  std::vector<BatchGroup> groups;  // widest clusters first
+  int clusterSize{1};              // the shape of the largest group (cfd_batch_shape)
   int threads{512};
-  int smemBytes{0};
   int lastIterations{0};
   cudaGraphExec_t graph{nullptr};  // the n-iteration launch, captured once
   int graphIterations{0};
@@ -1337,13 +1348,43 @@ namespace {
 cfd_status refreshTable(cfd_batch b) {
   std::vector<cfdb::Instance> table;
   table.reserve(b->handles.size());
-  for (cfd_handle h : b->handles) table.push_back(h->solver->deviceView());
+  for (const BatchGroup& g : b->groups) {
+    for (int k : g.members) table.push_back(b->handles[static_cast<std::size_t>(k)]->solver->deviceView());
+  }
   cudaError_t e = cudaMemcpyAsync(b->dTable, table.data(), table.size() * sizeof(cfdb::Instance),
                                   cudaMemcpyHostToDevice, b->stream);
   if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
   e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
   return CFD_OK;
+}
+
+/// n iterations of every solve of the batch, ordered on `s`: one launch per
+/// group, the groups forked from `s` onto their own streams and joined back,
+/// so solves of different launch shapes run side by side (a group of small
+/// clusters fills the SMs a group of wide ones leaves idle). Used directly
+/// and under stream capture.
+cfd_status launchGroups(cfd_batch b, int n, int stopStage, double tolerance, cudaStream_t s) {
+  if (b->groups.size() == 1) {
+    const BatchGroup& g = b->groups[0];
+    return cfdb::launchSimple(b->dTable + g.offset, g.count, g.clusterSize, g.threads, n, stopStage, tolerance, s,
+                              g.smemBytes);
+  }
+  cudaError_t e = cudaEventRecord(b->fork, s);
+  if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  cfd_status st = CFD_OK;
+  for (const BatchGroup& g : b->groups) {
+    e = cudaStreamWaitEvent(g.stream, b->fork, 0);
+    if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+    if (st == CFD_OK) {
+      st = cfdb::launchSimple(b->dTable + g.offset, g.count, g.clusterSize, g.threads, n, stopStage, tolerance,
+                              g.stream, g.smemBytes);
+    }
+    e = cudaEventRecord(g.done, g.stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, g.done, 0);
+    if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
+  }
+  return st;
 }
 }  // namespace
 
@@ -1360,17 +1401,45 @@ cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out
       return cfdb::fail(CFD_INVALID_ARGUMENT, "null solver in batch");
     }
     b->handles.push_back(solvers[k]);
-    b->clusterSize = std::max(b->clusterSize, solvers[k]->solver->clusterSize());
-    b->threads = solvers[k]->solver->threads();
   }
-  for (cfd_handle h : b->handles) {
-    b->smemBytes = std::max(b->smemBytes, h->solver->launchSmemBytes(b->clusterSize));
+  // One group per launch shape (each solve keeps its own), widest first so
+  // its clusters are placed before the narrower groups fill the gaps.
+  for (int k = 0; k < count; ++k) {
+    const cfdb::Solver& sv = *b->handles[static_cast<std::size_t>(k)]->solver;
+    auto it = std::find_if(b->groups.begin(), b->groups.end(), [&](const BatchGroup& g) {
+      return g.clusterSize == sv.clusterSize() && g.threads == sv.threads();
+    });
+    if (it == b->groups.end()) {
+      BatchGroup g;
+      g.clusterSize = sv.clusterSize();
+      g.threads = sv.threads();
+      b->groups.push_back(g);
+      it = b->groups.end() - 1;
+    }
+    it->members.push_back(k);
+    it->smemBytes = std::max(it->smemBytes, sv.launchSmemBytes(sv.clusterSize()));
   }
+  std::stable_sort(b->groups.begin(), b->groups.end(),
+                   [](const BatchGroup& a, const BatchGroup& c) { return a.clusterSize > c.clusterSize; });
+  int offset = 0;
+  std::size_t largest = 0;
+  for (std::size_t g = 0; g < b->groups.size(); ++g) {
+    b->groups[g].offset = offset;
+    b->groups[g].count = static_cast<int>(b->groups[g].members.size());
+    offset += b->groups[g].count;
+    if (b->groups[g].count > b->groups[largest].count) largest = g;
+  }
+  b->clusterSize = b->groups[largest].clusterSize;
+  b->threads = b->groups[largest].threads;
   cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&b->dTable), count * sizeof(cfdb::Instance));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (BatchGroup& g : b->groups) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) {
-    if (b->dTable) cudaFree(b->dTable);
-    delete b;
+    cfd_batch_destroy(b);
     return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
   }
   *out = b;
@@ -1385,8 +1454,7 @@ cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream) {
   }
   cudaStream_t s = (stream != nullptr) ? static_cast<cudaStream_t>(stream) : b->stream;
   b->lastIterations = n;
-  return cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize, b->threads, n,
-                            cfdb::kStageEnd, -1.0, s, b->smemBytes);
+  return launchGroups(b, n, cfdb::kStageEnd, -1.0, s);
 }
 
 cfd_status cfd_batch_graph_launch(cfd_batch b, int n, void* stream) {
@@ -1404,8 +1472,7 @@ cfd_status cfd_batch_graph_launch(cfd_batch b, int n, void* stream) {
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cfdb::fail(CFD_INITIALIZATION_FAILURE, cudaGetErrorString(e));
-    const cfd_status launched = cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize,
-                                                   b->threads, n, cfdb::kStageEnd, -1.0, b->stream, b->smemBytes);
+    const cfd_status launched = launchGroups(b, n, cfdb::kStageEnd, -1.0, b->stream);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(b->stream, &g);
     if (launched != CFD_OK) {
@@ -1461,10 +1528,7 @@ cfd_status cfd_batch_iterate(cfd_batch b, int n, double tol, int* taken, cfd_mon
     for (cfd_handle h : b->handles) {
       if (!h->solver->initialised()) return cfdb::fail(CFD_INVALID_ARGUMENT, "a solver in the batch is not initialised");
     }
-    if (cfd_status st = cfdb::launchSimple(b->dTable, static_cast<int>(b->handles.size()), b->clusterSize,
-                                           b->threads, chunk, cfdb::kStageEnd, tol, b->stream,
-                                           b->smemBytes);
-        st != CFD_OK) {
+    if (cfd_status st = launchGroups(b, chunk, cfdb::kStageEnd, tol, b->stream); st != CFD_OK) {
       return st;
     }
     if (cfd_status st = cfd_batch_monitors(b, ran.data(), last); st != CFD_OK) return st;
@@ -1489,10 +1553,18 @@ cfd_status cfd_batch_shape(cfd_batch b, int* clusterSize, int* threads) {
 
 cfd_status cfd_batch_destroy(cfd_batch b) {
   if (b == nullptr) return CFD_OK;
-  cudaStreamSynchronize(b->stream);
+  if (b->stream != nullptr) cudaStreamSynchronize(b->stream);
+  for (BatchGroup& g : b->groups) {
+    if (g.stream != nullptr) {
+      cudaStreamSynchronize(g.stream);
+      cudaStreamDestroy(g.stream);
+    }
+    if (g.done != nullptr) cudaEventDestroy(g.done);
+  }
   if (b->graph != nullptr) cudaGraphExecDestroy(b->graph);
-  cudaFree(b->dTable);
-  cudaStreamDestroy(b->stream);
+  if (b->dTable != nullptr) cudaFree(b->dTable);
+  if (b->fork != nullptr) cudaEventDestroy(b->fork);
+  if (b->stream != nullptr) cudaStreamDestroy(b->stream);
   delete b;
   return CFD_OK;
 }

@@ -393,10 +393,14 @@ cfd_status cfd_engine_destroy(cfd_engine e);
 /* ---- batches: many solves in one launch ------------------------------------
  * A batch is a descriptor table over existing handles (each keeps its own
  * device state). One launch runs every solve of the table, one thread-block
- * cluster each, so uneven sizes, angles and sections share the GPU. The
- * reference runs one solve per worker thread (src/app/SolverWorker.cpp); this
- * has no counterpart there. The handles must outlive the batch and must not
- * be iterated on their own while a batch launch is in flight. */
+ * cluster each, so uneven sizes, angles and sections share the GPU. Each
+ * solve keeps its own cluster size (set at create or by CFD_CLUSTER_SIZE);
+ * solves of different sizes run as one launch per size, side by side on
+ * streams forked from and joined back to the caller's, so small clusters can
+ * fill SMs that wide ones leave idle. The reference runs one solve per worker
+ * thread (src/app/SolverWorker.cpp); this has no counterpart there. The
+ * handles must outlive the batch and must not be iterated on their own while
+ * a batch launch is in flight. */
 typedef struct cfd_batch_t* cfd_batch;
 
 cfd_status cfd_batch_create(const cfd_handle* solvers, int count, cfd_batch* out);
@@ -415,7 +419,8 @@ cfd_status cfd_batch_launch(cfd_batch b, int n, void* stream);
 cfd_status cfd_batch_graph_launch(cfd_batch b, int n, void* stream);
 /* Monitors of the last launch (count entries); synchronises first. */
 cfd_status cfd_batch_monitors(cfd_batch b, int* taken, cfd_monitor* last);
-/* Cluster size (CTAs per solve) and threads per CTA used by launches. */
+/* Cluster size (CTAs per solve) and threads per CTA of the batch's largest
+ * group of solves. */
 cfd_status cfd_batch_shape(cfd_batch b, int* cluster_size, int* threads);
 cfd_status cfd_batch_destroy(cfd_batch b);
 

@@ -121,3 +121,44 @@ def test_graph_replayed_launches_equal_direct_launches():
         assert np.array_equal(a.read(f), b.read(f)), f
     ba.close()
     bb.close()
+
+
+def _sst_on(ctas, alpha):
+    mesh = cb.cgrid("0012", surface_points=64, wake_points=33, normal_points=49,
+                    first_layer_height=1e-5, upstream_chords=10.0, downstream_chords=15.0,
+                    vertical_chords=10.0)
+    with _env(CFD_CLUSTER_SIZE=ctas):
+        s = cb.SimpleSolver.create(mesh, cb.freestream_conditions(mesh, 1.0, alpha),
+                                   cb.Settings.defaults(inflow_viscosity_ratio=10.0))
+    s.set_turbulence_model(cb.MODEL_SST)
+    s.initialise(*cb.uniform_field(mesh, 1.0, alpha, 1.0, 1e6))
+    return s
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_a_batch_of_mixed_cluster_sizes_equals_each_solve_alone(graph):
+    # Solves created with different cluster sizes run as one launch per size,
+    # side by side on forked streams; each gives the bits it gives alone with
+    # its own size, directly or replayed from a captured graph.
+    shapes = [(16, 0.0), (8, 2.0), (4, 4.0), (8, 6.0), (16, 8.0)]
+    together = [_sst_on(r, a) for r, a in shapes]
+    batch = cb.Batch(together)
+    assert batch.shape()[0] in (8, 16)
+    for _ in range(6):
+        if graph:
+            batch.graph_launch(1)
+        else:
+            batch.launch(1)
+    batch.monitors()
+    batch.close()
+    for (r, a), s in zip(shapes, together):
+        alone = _sst_on(r, a)
+        solo = cb.Batch([alone])
+        for _ in range(6):
+            solo.launch(1)
+        solo.monitors()
+        solo.close()
+        for f in FIELDS:
+            assert np.array_equal(s.read(f), alone.read(f)), (r, a, f)
+        alone.close()
+        s.close()
