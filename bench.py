@@ -530,7 +530,7 @@ def run_ours(args) -> None:
             "roofline": roofline,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps, "clocks": clocks, "finite": finite,
+            "gpu_launches": args.steps * len(config["cluster_sizes"]), "clocks": clocks, "finite": finite,
         }
         if mixed is not None:
             m_value = all_cells * args.steps / times[2]
