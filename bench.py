@@ -63,7 +63,7 @@ POLAR = ([("2412", float(a), 3e6, "fine", 5e-6) for a in range(-4, 17)]
             ("0012", 4.0, 1e6, "fine", 5e-6)])
 POLAR_NAME = ("batched polar: NACA2412 k-omega SST Re3e6 C-grid 768x192, alpha -4..16 step 1 "
               "(21 solves) + NACA0012 k-omega SST Re1e6 alpha 4 on 192x48/384x96/768x192, "
-              "24 solves in one launch")
+              "24 solves in one batch (one launch per cluster size)")
 # The mixed form runs on clusters of at most 8 CTAs (the engine's default
 # policy for it: smaller clusters fit more of its solves on the GPU).
 MIXED_CLUSTER = 8
