@@ -59,6 +59,7 @@ constexpr int kFlagOnePassCg = 16;
 constexpr int kFlagBarrierSweeps = 32;
 constexpr int kFlagSharedCg = 128;  // the pressure CG's band in shared memory where it fits
 constexpr int kFlagChainWaitTest = 64;  // tests only: a chained stage also waits for a count nothing sets
+constexpr int kFlagHaloWaitTest = 256;  // tests only: the split CG also waits once for a count nothing sets
 
 // Fault codes a launch leaves in iterations[1] (bits, or-ed together).
 constexpr int kFaultChainWait = 1;  // a chained k/omega sweep stage gave up waiting for its neighbour

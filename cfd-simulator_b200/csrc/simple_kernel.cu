@@ -1741,7 +1741,8 @@ __host__ __device__ inline long long cgSplitSmemDoubles(int NI, int NJ, int R) {
 /// order as cgGlobal and cgShared, so the same bits. A halo wait that gives
 /// up sets kFaultHaloWait in the launch's fault word and the solve carries
 /// on without waiting again.
-DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double gamma) {
+DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, double initial, double gamma,
+                      bool waitTest) {
   const int NI = I.NI, NJ = I.NJ;
   const int R = static_cast<int>(t.R), rank = static_cast<int>(t.rank);
   const double* __restrict__ pD = I.pD;
@@ -1856,6 +1857,13 @@ DEV int cgGlobalSplit(const Instance& I, Team& t, Shared& sh, double* dyn, doubl
     // the neighbours' rows of this iteration (pushed in their pass 1); then
     // the barrier is armed for the next iteration's, before this CTA can
     // reach the reduction after which the neighbours push them
+    if (threadIdx.x == 0 && waitTest && iter == 0) {
+      // test: the first iteration also waits for a count nothing sets
+      long long spins = 0;
+      while (loadRelaxedCluster(&sh.chainNever) == 0u && ++spins <= kChainSpinLimit) {
+      }
+      if (spins > kChainSpinLimit) atomicOr(I.iterations + 1, kFaultHaloWait);
+    }
     if (threadIdx.x == 0) {
       long long spins = 0;
       while (!haloFaulted && !mbarDone(&sh.haloBar, sh.haloPhase & 1u)) {
@@ -2130,7 +2138,7 @@ simpleKernel(const Instance* __restrict__ instances, int iterations, int stopSta
         cgIters = cgShared(I, t, sh, dyn, initial, rz);
       } else if (initial > 0.0 && !(flags & kFlagOnePassCg) && I.NJ >= static_cast<int>(t.R) &&
                  cgSplitSmemDoubles(I.NI, I.NJ, static_cast<int>(t.R)) * 8 <= smemBytes) {
-        cgIters = cgGlobalSplit(I, t, sh, dyn, initial, rz);
+        cgIters = cgGlobalSplit(I, t, sh, dyn, initial, rz, (flags & kFlagHaloWaitTest) != 0);
       } else if (initial > 0.0) {
         cgIters = cgGlobal(I, t, sh, initial, rz);
       }
@@ -2306,7 +2314,8 @@ int kernelFlags() {
   // identical results); bit 3 runs the reference's two-reduction CG instead
   // of the single-reduction one (the same to rounding). Bit 6 is for tests:
   // a chained k/omega stage also waits for a count that nothing sets, so
-  // that wait gives up and the launch reports its fault word.
+  // that wait gives up and the launch reports its fault word; bit 8 does the
+  // same for the two-pass pressure CG's halo wait.
   const char* env = std::getenv("CFD_KERNEL_FLAGS");
   return (env != nullptr) ? std::atoi(env) : 0;
 }

@@ -73,6 +73,19 @@ def test_a_chain_wait_that_gives_up_is_reported_and_the_device_stays_usable():
     assert np.all(np.isfinite(ha)) and np.array_equal(ha, hb)
 
 
+def test_a_halo_wait_that_gives_up_is_reported_and_the_device_stays_usable():
+    # flag bit 8 makes the two-pass pressure CG's first iteration also wait
+    # for a count that nothing sets: that wait gives up after its poll limit,
+    # the halo rows still arrive, the launch finishes, and the host reads the
+    # fault word as an error.
+    with pytest.raises(cb.CfdError) as err:
+        _medium_sst(1, 256)
+    assert err.value.code == 8  # CFD_INTERNAL
+    assert "halo row" in str(err.value)
+    a, ha = _medium_sst(2, 0)
+    assert np.all(np.isfinite(ha))
+
+
 def test_shared_and_global_memory_cg_are_bit_identical():
     # 384 x 96 on 16 CTAs: the pressure CG runs from global memory in two
     # passes by default and keeps its band in shared memory with flag bit 7;
