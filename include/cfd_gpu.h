@@ -35,7 +35,9 @@ enum {
   CFD_NOT_IMPLEMENTED = 5,
   CFD_INITIALIZATION_FAILURE = 6, /* also: CUDA device or allocation failure */
   CFD_NUMERICAL_FAILURE = 7,
-  CFD_INTERNAL = 8
+  CFD_INTERNAL = 8 /* also: a bounded wait between a solve's CTAs gave up
+                     (cfd_last_error says which); that launch's results are
+                     not valid, and the device stays usable */
 };
 
 typedef struct cfd_solver_t* cfd_handle;
