@@ -10,7 +10,6 @@ same mesh, and checks the converged fields (1e-9 relative L2), the turbulence
 model's fields and y+, and Cl/Cd/Cm from the reference's own extractSurface
 and integrateForces (1e-7 relative), plus move-only ownership, the error-code
 mapping and the mutable field() round trip."""
-import json
 import os
 import subprocess
 
@@ -22,10 +21,13 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "shim_check")
 
 
 def _reference_include():
+    """The reference checkout's include directory, from the oracle recipe's REF."""
     try:
-        with open(os.path.join(ROOT, "BASELINE.json")) as f:
-            path = json.load(f)["reference_path"]
-    except (OSError, KeyError, ValueError):
+        path = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                              capture_output=True, text=True, check=True).stdout.strip()
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    if not path:
         return None
     inc = os.path.join(path, "include")
     return inc if os.path.isdir(os.path.join(inc, "cfd", "solver")) else None
