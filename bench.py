@@ -547,6 +547,9 @@ def run_ours(args) -> None:
             line["cpu_baseline"] = cpu_baseline()
         if world == 1 and not args.no_convergence and not c2:
             line["polar"] = polar_to_tolerance(cb, args.tolerance, args.cap, args.chunk)
+            if "cpu_baseline" in line:
+                line["polar"]["reference_cpu_estimate"] = reference_polar_estimate(
+                    line["polar"]["plain"]["points"], line["cpu_baseline"])
         print(json.dumps(line), flush=True)
     if mixed is None:
         batch.close()
@@ -601,6 +604,24 @@ def _polar_requests(cb, tolerance, cap, precision):
                                surface_points=sp, wake_points=wp, normal_points=npn,
                                first_layer_height=fl, settings=settings))
     return reqs
+
+
+def reference_polar_estimate(points, cpu: dict) -> dict:
+    """The reference's solves/min on the same polar, estimated rather than run
+    (a run would take hours): the plain form's iteration counts per point
+    (the reference's algorithm, which it follows to rounding) times the
+    point's cells, at the reference's measured cell-iterations/s per host
+    core, scheduled longest first over the cores it was measured on."""
+    cores = int(cpu["cores"])
+    rate = float(cpu["value"]) / cores  # cell-iterations/s of one core
+    loads = [0.0] * cores
+    for work in sorted((p["iterations"] * p["cells"] / rate for p in points), reverse=True):
+        k = loads.index(min(loads))
+        loads[k] += work
+    wall = max(loads)
+    return {"solves_per_min": 60.0 * len(points) / wall, "wall_s": wall, "cores": cores,
+            "basis": "estimate: plain-form iterations x cells per point at the reference's measured "
+                     "cell-iterations/s per core (cpu_baseline), longest first over the cores; not a timed run"}
 
 
 def polar_to_tolerance(cb, tolerance, cap, chunk, forms=("plain", "mixed"), csv_prefix=""):
